@@ -1,0 +1,484 @@
+#!/usr/bin/env python
+"""Benchmark driver: prints ONE JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload u1_microbench]
+
+Workload "u1_microbench": the U(1) kernel microbenchmark -- rank-4 float64
+tensors whose legs carry charges -4..4 with degeneracies ~ exp(-q^2/8) rounded
+(largest remainder) to 256 states per leg, only charge-conserving blocks filled
+with seeded N(0,1) entries (17 blocks, 455 018 564 coefficients, 3.64 GB per
+tensor).  One step = permute (0,2),(1,3) then the grouped matmul against a
+second tensor of the same structure, the hot path of every CTMRG contraction.
+Inputs are larger than the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path does not shard -- every rank runs an independent replica
+(weak scaling), and the timed region is the max over ranks.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+LEG_STATES = 256
+QMAX = 4
+SEED = 2024
+
+
+def microbench_rep(total, qmax=QMAX):
+    """Charges -qmax..qmax, degeneracy ~ exp(-q^2/8) with largest-remainder
+    rounding to `total` states, sorted by charge."""
+    q = np.arange(-qmax, qmax + 1)
+    w = np.exp(-(q**2) / 8.0)
+    raw = w / w.sum() * total
+    deg = np.floor(raw).astype(int)
+    rem = total - deg.sum()
+    order = np.argsort(-(raw - deg), kind="stable")
+    deg[order[:rem]] += 1
+    return np.repeat(q, deg).astype(np.int8)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi missing"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9], strict=True):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ---------------------------------------------------------------- workloads
+
+
+class U1Microbench:
+    name = "u1_microbench"
+
+    def __init__(self, leg_states=LEG_STATES):
+        from frostspin_b200 import U1SymmetricTensor
+
+        self.cls = U1SymmetricTensor
+        rep = microbench_rep(leg_states)
+        self.rep = rep
+        self.sig1 = np.array([False, False, True, True])
+        self.sig2 = np.array([True, False, False, True])
+        self.irr1, self.shapes1 = U1SymmetricTensor.get_block_sizes(
+            (rep, rep), (rep, rep), self.sig1)
+        self.irr2, self.shapes2 = U1SymmetricTensor.get_block_sizes(
+            (rep, rep), (rep, rep), self.sig2)
+        self.ncoeff = int((self.shapes1[:, 0] * self.shapes1[:, 1]).sum())
+
+    def device_inputs(self):
+        import torch
+
+        g = torch.Generator(device="cuda")
+        g.manual_seed(SEED)
+        n2 = int((self.shapes2[:, 0] * self.shapes2[:, 1]).sum())
+        f1 = torch.randn(self.ncoeff, dtype=torch.float64, device="cuda", generator=g)
+        f2 = torch.randn(n2, dtype=torch.float64, device="cuda", generator=g)
+        rep = self.rep
+        t1 = self.cls.from_flat((rep, rep), (rep, rep), f1, self.irr1, self.sig1)
+        t2 = self.cls.from_flat((rep, rep), (rep, rep), f2, self.irr2, self.sig2)
+        return t1, t2
+
+    def flops(self, p, t2):
+        common, i1, i2 = np.intersect1d(p.block_irreps, t2.block_irreps,
+                                        return_indices=True)
+        m = p.block_shapes[i1, 0]
+        k = p.block_shapes[i1, 1]
+        n = t2.block_shapes[i2, 1]
+        return float((2 * m * k * n).sum())
+
+    @staticmethod
+    def step(t1, t2, ev=None):
+        if ev is not None:
+            ev[0].record()
+        p = t1.permute((0, 2), (1, 3))
+        if ev is not None:
+            ev[1].record()
+        m = p @ t2
+        if ev is not None:
+            ev[2].record()
+        return m
+
+
+def measure_dgemm_peak():
+    """cuBLAS DGEMM throughput (TFLOP/s) on 8192^3, best of 3: the measured FP64
+    denominator for the FP64 GEMM roofline."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n**3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+# --------------------------------------------------------------- CPU baseline
+
+
+def cpu_microbench_seconds(leg_states, nthreads):
+    """Oracle (numpy restatement of the reference) permute + matmul on a reduced
+    microbench; returns (t_permute, t_matmul, ncoeff, flops) of the sample."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(nthreads))
+    from oracle import frostspin_oracle as fo
+
+    rep = microbench_rep(leg_states)
+    rng = np.random.default_rng(SEED)
+    sig1 = np.array([False, False, True, True])
+    irr, shapes = fo.get_block_sizes((rep, rep), (rep, rep), sig1)
+    t1 = fo.OTensor((rep, rep), (rep, rep), [rng.standard_normal(tuple(s)) for s in shapes],
+                    irr, sig1)
+    sig2 = np.array([True, False, False, True])
+    irr2, shapes2 = fo.get_block_sizes((rep, rep), (rep, rep), sig2)
+    t2 = fo.OTensor((rep, rep), (rep, rep), [rng.standard_normal(tuple(s)) for s in shapes2],
+                    irr2, sig2)
+    t0 = time.perf_counter()
+    p = fo.permute(t1, (0, 2), (1, 3))
+    t1_ = time.perf_counter()
+    fo.matmul(p, t2)
+    t2_ = time.perf_counter()
+    ncoeff = sum(b.size for b in t1.blocks)
+    flops = 0.0
+    for q, b in zip(p.block_irreps, p.blocks, strict=True):
+        j = np.flatnonzero(t2.block_irreps == q)
+        if j.size:
+            flops += 2.0 * b.shape[0] * b.shape[1] * t2.blocks[j[0]].shape[1]
+    return t1_ - t0, t2_ - t1_, ncoeff, flops
+
+
+def cpu_baseline_full_step(full_ncoeff, full_flops, sample_states=128):
+    nthreads = os.cpu_count() or 1
+    tp, tm, nc, fl = cpu_microbench_seconds(sample_states, nthreads)
+    t_full = tp * full_ncoeff / nc + tm * full_flops / fl
+    return t_full, {
+        "cores": nthreads,
+        "kind": "port",
+        "sample": (
+            f"oracle numpy restatement of the reference permute+matmul on the same "
+            f"microbench with {sample_states}-state legs ({nc} coeff, {fl:.3g} flop): "
+            f"permute {tp:.3f} s, matmul {tm:.3f} s, scaled to the full step by "
+            f"coefficients (permute) and flops (matmul)"
+        ),
+    }
+
+
+# ------------------------------------------------------------------- driver
+
+
+def dist_init(gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from frostspin_b200 import _native
+
+    wl = U1Microbench()
+    t1, t2 = wl.device_inputs()
+    m = wl.step(t1, t2)
+    flops = wl.flops(t1.permute((0, 2), (1, 3)), t2)
+    del m
+    for _ in range(args.warmup):
+        wl.step(t1, t2)
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for k in range(args.steps):
+        wl.step(t1, t2, evs[k])
+    end.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    elapsed = max_over_ranks(start.elapsed_time(end) * 1e-3, world)
+    perm_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    gemm_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+
+    # end-to-end through the public API from pinned host buffers
+    rep = wl.rep
+    h1 = t1.data.cpu().pin_memory()
+    h2 = t2.data.cpu().pin_memory()
+    out_host = torch.empty(int(t1.data.numel()), dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    barrier(world)
+    es = torch.cuda.Event(enable_timing=True)
+    ee = torch.cuda.Event(enable_timing=True)
+    es.record()
+    for _ in range(e2e_steps):
+        a = wl.cls.from_flat((rep, rep), (rep, rep), h1, wl.irr1, wl.sig1)
+        b = wl.cls.from_flat((rep, rep), (rep, rep), h2, wl.irr2, wl.sig2)
+        r = wl.step(a, b)
+        out_host[: r.data.numel()].copy_(r.data, non_blocking=True)
+        del a, b, r
+    ee.record()
+    torch.cuda.synchronize()
+    e2e_elapsed = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
+
+    hbm, _bf16, peak_kind = load_peaks()
+    fp64_peak = measure_dgemm_peak()
+    perm_bytes = 16.0 * wl.ncoeff
+    perm_gbs = perm_bytes / (perm_ms * 1e-3) / 1e9
+    gemm_tf = flops / (gemm_ms * 1e-3) / 1e12
+    value = world * args.steps / elapsed
+    line = {
+        "metric": "U(1) microbench permute+grouped-matmul steps/s",
+        "value": value,
+        "unit": "step/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) blocks)",
+        "impl": "ours",
+        "config": {
+            "workload": wl.name,
+            "legs": "4 x 256 states, U(1) charges -4..4, degeneracies [7,17,32,46,52,46,32,17,7]",
+            "ncoeff": wl.ncoeff,
+            "gemm_flop_per_step": flops,
+            "gemm_precision": "fp64",
+            "l2": "inputs 3.64 GB per tensor > 126 MB L2; no flush needed",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {
+            "bound": "tensor",
+            "kernel": "k_grouped_dgemm",
+            "achieved": gemm_tf,
+            "peak": fp64_peak,
+            "unit": "TFLOP/s",
+            "frac": gemm_tf / fp64_peak,
+            "peak_kind": "measured in-run cuBLAS DGEMM 8192^3 (no FP64 figure in the peaks file)",
+            "traffic": None,
+        },
+        "roofline_permute": {
+            "bound": "hbm",
+            "kernel": "k_perm_gather",
+            "achieved": perm_gbs,
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": perm_gbs / hbm,
+            "peak_kind": f"{peak_kind} copy bandwidth",
+            "ms": perm_ms,
+        },
+        "e2e": {
+            "value": world * e2e_steps / e2e_elapsed,
+            "unit": "step/s",
+            "h2d_bytes_per_step": int(h1.numel() * 8 + h2.numel() * 8),
+            "d2h_bytes_per_step": int(t1.data.numel() * 8),
+        },
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        t_cpu, info = cpu_baseline_full_step(wl.ncoeff, flops)
+        info["value"] = 1.0 / t_cpu
+        info["unit"] = "step/s"
+        line["cpu_baseline"] = info
+    del _native
+    return line
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    wl_states = LEG_STATES
+    from frostspin_b200.symmetric_tensor.abelian_plan import GroupInfo  # noqa: F401
+
+    rep = microbench_rep(wl_states)
+    from oracle import frostspin_oracle as fo
+
+    sig1 = np.array([False, False, True, True])
+    irr, shapes = fo.get_block_sizes((rep, rep), (rep, rep), sig1)
+    ncoeff = int((shapes[:, 0] * shapes[:, 1]).sum())
+    # flops of the full step from block shapes (permuted blocks are square)
+    sigp = np.array([False, True, False, True])
+    irrp, shp = fo.get_block_sizes((rep, rep), (rep, rep), sigp)
+    flops = float((2 * shp[:, 0] * shp[:, 1] * shp[:, 1]).sum())
+    times = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        t, info = cpu_baseline_full_step(ncoeff, flops)
+        if i >= args.warmup:
+            times.append(t)
+    value = 1.0 / float(np.mean(times))
+    info["value"] = value
+    info["unit"] = "step/s"
+    return {
+        "metric": "U(1) microbench permute+grouped-matmul steps/s",
+        "value": value,
+        "unit": "step/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) blocks)",
+        "impl": "reference",
+        "config": {"workload": "u1_microbench", "ncoeff": ncoeff,
+                   "gemm_flop_per_step": flops},
+        "cpu_baseline": info,
+        "e2e": {"value": value, "unit": "step/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["u1_microbench"], default="u1_microbench")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    world, rank, local = dist_init(args.gpus)
+    line = run_ours(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,164 @@
+"""ctypes binding of the frostspin_b200 C ABI (include/frostspin_b200.h).
+
+The shared library is built in-tree by ``frostspin_b200.build``.  There is no
+fallback: if the library is missing or a CUDA device is absent, every device
+operation raises.  Plan tables are numpy structured arrays whose dtypes mirror
+the C structs byte for byte (checked by tests/test_abi.py against the header
+compiled with gcc); they are uploaded once into torch-owned device buffers.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(__file__), "_lib", "libfrostspin_b200.so")
+
+FS_OK = 0
+FS_PERM_MAXR = 8
+
+# ----------------------------------------------------------------- C struct dtypes
+PERM_EB_DTYPE = np.dtype(
+    [
+        ("obase", "<i8"),
+        ("nbase", "<i8"),
+        ("ostride", "<i8", (FS_PERM_MAXR,)),
+        ("nstride", "<i8", (FS_PERM_MAXR,)),
+        ("dims", "<u4", (FS_PERM_MAXR,)),
+        ("divm", "<u4", (FS_PERM_MAXR,)),
+        ("divs", "<u4", (FS_PERM_MAXR,)),
+        ("ndim", "<i4"),
+        ("volume", "<u4"),
+        ("tile_leg", "<i4"),
+        ("pad", "<i4"),
+    ]
+)
+
+PERM_TASK_DTYPE = np.dtype(
+    [("eb", "<i4"), ("start", "<u4"), ("count", "<u4"), ("pad", "<u4")]
+)
+
+GEMM_PROBLEM_DTYPE = np.dtype(
+    [
+        ("A", "<u8"),
+        ("B", "<u8"),
+        ("C", "<u8"),
+        ("lda", "<i8"),
+        ("ldb", "<i8"),
+        ("ldc", "<i8"),
+        ("M", "<i4"),
+        ("N", "<i4"),
+        ("K", "<i4"),
+        ("transA", "<i4"),
+        ("transB", "<i4"),
+        ("pad", "<i4"),
+        ("alpha", "<f8"),
+        ("beta", "<f8"),
+    ]
+)
+
+GEMM_TILE_DTYPE = np.dtype(
+    [("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")]
+)
+
+SEGMENT_DTYPE = np.dtype([("offset", "<i8"), ("length", "<i8"), ("weight", "<f8")])
+
+PAIR_BLOCK_DTYPE = np.dtype(
+    [
+        ("a_off", "<i8"),
+        ("b_off", "<i8"),
+        ("m", "<i4"),
+        ("n", "<i4"),
+        ("a_trans", "<i4"),
+        ("b_trans", "<i4"),
+        ("weight", "<f8"),
+    ]
+)
+
+DIAG_BLOCK_DTYPE = np.dtype(
+    [
+        ("x_off", "<i8"),
+        ("out_off", "<i8"),
+        ("d_off", "<i8"),
+        ("m", "<i4"),
+        ("n", "<i4"),
+        ("x_trans", "<i4"),
+        ("left", "<i4"),
+    ]
+)
+
+# name -> (restype, argtypes); pointers and streams travel as c_void_p
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I32 = ctypes.c_int32
+_D = ctypes.c_double
+SIGNATURES = {
+    "fs_version": (ctypes.c_int, []),
+    "fs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "fs_last_cuda_error": (ctypes.c_char_p, []),
+    "fs_abelian_permute": (
+        ctypes.c_int,
+        [_P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
+    ),
+    "fs_dgemm_tile_shape": (ctypes.c_int, [_P, _P]),
+    "fs_grouped_dgemm": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
+    "fs_scale": (ctypes.c_int, [_P, _I64, _D, _P]),
+    "fs_axpby": (ctypes.c_int, [_P, _P, _I64, _D, _D, _P]),
+    "fs_pow": (ctypes.c_int, [_P, _P, _I64, _D, _P]),
+    "fs_reduce_partials": (ctypes.c_int, []),
+    "fs_weighted_sumsq": (ctypes.c_int, [_P, _P, _I64, _P, _I64, _P, _P]),
+    "fs_weighted_sum": (ctypes.c_int, [_P, _P, _I64, _P, _I64, _P, _P]),
+    "fs_pair_contract": (ctypes.c_int, [_P, _P, _P, _I64, _P, _I64, _P, _P]),
+    "fs_diag_mul": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
+}
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    """A frostspin_b200 C ABI call returned a non-zero status."""
+
+
+def lib():
+    """Load the shared library once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            msg = (
+                f"frostspin_b200 CUDA library not found at {LIB_PATH}; build it with "
+                "`python -m frostspin_b200.build`"
+            )
+            raise NativeError(msg)
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status, what):
+    if status != FS_OK:
+        text = lib().fs_status_string(status).decode()
+        cuda = lib().fs_last_cuda_error().decode()
+        msg = f"{what} failed: status {status} ({text}); last CUDA error: {cuda}"
+        raise NativeError(msg)
+
+
+def call(name, *args):
+    """Call a C ABI function by name and raise on a non-zero status."""
+    st = getattr(lib(), name)(*args)
+    check(st, name)
+    return st
+
+
+def reduce_partials():
+    return int(lib().fs_reduce_partials())
+
+
+def dgemm_tile_shape():
+    tm = ctypes.c_int32()
+    tn = ctypes.c_int32()
+    call("fs_dgemm_tile_shape", ctypes.byref(tm), ctypes.byref(tn))
+    return tm.value, tn.value

@@ -1,0 +1,109 @@
+"""C4v-symmetric classical CTMRG on the square lattice (single layer).
+
+Mirrors examples/ising_classical_ctmrg.py:115-304 (iterate_ctm, env_1site,
+env_2sites) of the reference: the corner is kept as its eigenvalue spectrum s
+(a DiagonalTensor) and the edge as T (chi, D, chi).  Works for any abelian
+device SymmetricTensor; the Ising site tensors are built in the Z2 basis
+exactly as the reference example does (:44-64, :362-384).
+"""
+
+import numpy as np
+import scipy.linalg as lg
+
+from ..symmetric_tensor import DiagonalTensor, U1SymmetricTensor
+
+
+def iterate_c4v(s, T, a, a2, chi_target):
+    """One C4v CTMRG iteration (examples/ising_classical_ctmrg.py:115-204)."""
+    Tp = T.permute((0, 1), (2,))
+    matC = Tp * s
+    matC = matC @ T
+    matC = matC.permute((1, 2), (0, 3))
+    matC = a2 @ matC
+    matC = matC.permute((0, 2), (1, 3))
+    news, U = matC.truncated_eigh(chi_target)
+    news /= news.norm()
+    newT = U.permute((1,), (0, 2))
+    newT = Tp @ newT
+    newT = newT.permute((1, 2), (0, 3))
+    newT = a @ newT
+    newT = newT.permute((0, 2), (1, 3))
+    newT = U.dagger() @ newT
+    newT /= newT.norm()
+    return news, newT
+
+
+def env_1site(s, T):
+    """examples/ising_classical_ctmrg.py:207-251."""
+    Tp = T.permute((0, 1), (2,))
+    corner = Tp * s
+    half = corner @ corner.permute((0,), (1, 2))
+    left = half.permute((1, 2), (0, 3))
+    right = half.permute((3, 0), (1, 2))
+    full = left @ right
+    return full.permute((0, 3), (2, 1))
+
+
+def env_2sites(s, T):
+    """examples/ising_classical_ctmrg.py:254-304."""
+    Tp = T.permute((0, 1), (2,))
+    env = Tp * s
+    env = env @ env.permute((0,), (1, 2))
+    env = Tp @ env.permute((0,), (1, 2, 3))
+    left = env.permute((1, 2, 3), (0, 4))
+    right = env.permute((4, 0), (1, 2, 3))
+    return left @ right
+
+
+def ising_site_tensors(beta):
+    """Z2-basis Ising tensors (a, a2) plus dense a0 and the magnetisation
+    operator in the same basis (examples/ising_classical_ctmrg.py:44-64,
+    :362-384)."""
+    d = 2
+    h = -2 * np.eye(2) + 1
+    sq_bw = lg.sqrtm(np.exp(-beta * h)).real
+    delta = np.zeros((d,) * 4)
+    delta[0, 0, 0, 0] = delta[1, 1, 1, 1] = 1
+    a0 = np.einsum("abcd,ai,bj,ck,dl->ijkl", delta, sq_bw, sq_bw, sq_bw, sq_bw)
+    mop = delta.copy()
+    mop[1, 1, 1, 1] = -1
+    mop = np.einsum("abcd,ai,bj,ck,dl->ijkl", mop, sq_bw, sq_bw, sq_bw, sq_bw)
+    K = np.array([[-1.0, 1.0], [1.0, 1.0]]) / np.sqrt(2)
+    a0d = np.einsum("abcd,ai,bj,ck,dl->ijkl", a0, K, K, K, K)
+    mopd = np.einsum("abcd,ai,bj,ck,dl->ijkl", mop, K, K, K, K)
+    rep = np.array([-128, 0], dtype=np.int8)
+    siga = np.array([False, False, True, True])
+    a = U1SymmetricTensor.from_array(a0d, (rep, rep), (rep, rep), signature=siga)
+    siga2 = np.array([False, True, True, True])
+    a2 = U1SymmetricTensor(a.row_reps, a.col_reps, a.blocks, a.block_irreps, siga2)
+    return a, a2, a0d, mopd
+
+
+def ising_initial_environment(chi, rng):
+    """Seeded Z2 corner spectrum and symmetric edge tensor
+    (examples/ising_classical_ctmrg.py:386-412)."""
+    d0o = d0e = chi // 2
+    s_odd = rng.normal(size=(d0o,))
+    s_odd = s_odd[np.abs(s_odd).argsort()[::-1]] / lg.norm(s_odd)
+    s_even = rng.normal(size=(d0e,))
+    s_even = s_even[np.abs(s_even).argsort()[::-1]] / lg.norm(s_even)
+    corner = np.array([-128] * d0o + [0] * d0e, dtype=np.int8)
+    s = DiagonalTensor(
+        (s_odd, s_even), corner, np.array([-128, 0], dtype=np.int8), [1, 1], "U1"
+    )
+    rep = np.array([-128, 0], dtype=np.int8)
+    sigT = np.array([False, False, True])
+    T = U1SymmetricTensor.random((corner,), (rep, corner), signature=sigT, rng=rng)
+    temp = U1SymmetricTensor((corner,), (rep, corner), T.blocks, T.block_irreps, [1, 0, 0])
+    T = T + temp.permute((2,), (1, 0))
+    T /= T.norm()
+    return s, T
+
+
+def energy_per_bond(s, T, a0d, mopd):
+    """-<s_i s_j> on one bond from the two-site environment; the reference
+    example prints the per-site energy, 2 bonds (:344-350)."""
+    env2 = env_2sites(s, T).toarray()
+    nr = np.einsum("abcdef,bgdc,afeg->", env2, a0d, a0d)
+    sdsr = np.einsum("abcdef,bgdc,afeg->", env2, mopd, mopd)
+    return -sdsr / nr

@@ -1,0 +1,64 @@
+"""Device plumbing: the CUDA device, the current stream, table uploads and scratch.
+
+PyTorch only provides memory, streams and host<->device copies here; every
+computation on symmetric-tensor data goes through the C ABI in ``_native``.
+"""
+
+import numpy as np
+import torch
+
+from . import _native
+
+_scratch = {}
+
+
+def device():
+    """The CUDA device tensors live on.  Raises when CUDA is unavailable: there is
+    no CPU fallback for any symmetric-tensor operation."""
+    if not torch.cuda.is_available():
+        msg = "frostspin_b200 needs a CUDA device (B200, sm_100a); none is available"
+        raise RuntimeError(msg)
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream():
+    """cudaStream_t of torch's current stream, as an integer handle."""
+    return torch.cuda.current_stream().cuda_stream
+
+
+def ptr(t):
+    return t.data_ptr() if t is not None and t.numel() > 0 else None
+
+
+def upload(arr):
+    """Copy a numpy array (any dtype, structured included) into a new uint8 device
+    buffer; the result owns its memory and must outlive the kernels reading it."""
+    a = np.ascontiguousarray(arr)
+    raw = torch.from_numpy(a.view(np.uint8).reshape(-1))
+    if raw.numel() == 0:
+        return torch.empty(0, dtype=torch.uint8, device=device())
+    return raw.to(device(), non_blocking=False)
+
+
+def upload_f64(arr):
+    a = np.ascontiguousarray(arr, dtype=np.float64)
+    return torch.from_numpy(a).to(device())
+
+
+def scratch_partials():
+    """Per-device scratch for two-pass reductions (fs_reduce_partials() doubles)."""
+    dev = device()
+    key = ("partials", dev.index)
+    buf = _scratch.get(key)
+    if buf is None:
+        buf = torch.empty(_native.reduce_partials(), dtype=torch.float64, device=dev)
+        _scratch[key] = buf
+    return buf
+
+
+def empty_f64(n):
+    return torch.empty(int(n), dtype=torch.float64, device=device())
+
+
+def zeros_f64(n):
+    return torch.zeros(int(n), dtype=torch.float64, device=device())

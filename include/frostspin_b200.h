@@ -1,0 +1,212 @@
+/*
+ * frostspin_b200 C ABI.
+ *
+ * Block-sparse symmetric-tensor kernels for NVIDIA B200 (sm_100a).  Every entry
+ * point takes plain device pointers, sizes and a cudaStream_t passed as void*,
+ * returns an int status (FS_OK == 0, negative on error) and never allocates or
+ * frees device memory: the caller (PyTorch's caching allocator in the Python
+ * package) owns every buffer, including plan tables and scratch space.  No
+ * exception crosses this boundary.
+ *
+ * Data layout shared by all entry points: a symmetric tensor is one contiguous
+ * float64 buffer holding its irrep blocks back to back, each block a dense
+ * row-major (C-order) matrix at an element offset into the buffer.  A tensor
+ * may instead carry all of its blocks transposed (F-order); the plans below
+ * encode that in their strides.
+ *
+ * Each declaration names the reference (frostspin 1.0.0) interface it replaces.
+ */
+#ifndef FROSTSPIN_B200_H
+#define FROSTSPIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define FS_OK 0
+#define FS_ERR_INVALID_ARG (-1)   /* null pointer, negative size, bad enum       */
+#define FS_ERR_LAUNCH (-2)        /* kernel launch failed (cudaGetLastError)     */
+#define FS_ERR_BOUNDS (-3)        /* a plan entry lies outside its buffer        */
+#define FS_ERR_TIMEOUT (-4)       /* a bounded device wait ran out               */
+#define FS_ERR_UNSUPPORTED (-5)   /* shape or mode this build does not handle    */
+#define FS_ERR_CUDA (-6)          /* other CUDA runtime error                    */
+#define FS_ERR_TOO_LARGE (-7)     /* request exceeds a fixed internal capacity   */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int fs_version(void);
+
+/* Human-readable text of a status code (static storage). */
+const char* fs_status_string(int status);
+
+/* Name of the last CUDA error seen by this library on the calling thread. */
+const char* fs_last_cuda_error(void);
+
+/* --------------------------------------------------------- abelian permute */
+/*
+ * An elementary block (EB) is the set of tensor entries whose legs each lie in
+ * one fixed run of constant irrep ("segment") of their representation.  Inside
+ * one EB the input and output element offsets are affine in the per-leg local
+ * indices, so the whole permutation is a batch of strided copies.  Legs are
+ * listed outer to inner in output order; dims[ndim-1] is the output-innermost
+ * leg.  divm/divs are the Granlund-Montgomery magic multiplier and shift for
+ * dividing by dims[k] (host computed).  obase < 0 marks an EB whose source
+ * block is absent: its output entries are written as zeros.
+ */
+#define FS_PERM_MAXR 8
+
+typedef struct FsPermEB {
+    int64_t obase;                   /* input element offset of local index 0   */
+    int64_t nbase;                   /* output element offset of local index 0  */
+    int64_t ostride[FS_PERM_MAXR];   /* input stride per leg (elements)         */
+    int64_t nstride[FS_PERM_MAXR];   /* output stride per leg (elements)        */
+    uint32_t dims[FS_PERM_MAXR];
+    uint32_t divm[FS_PERM_MAXR];
+    uint32_t divs[FS_PERM_MAXR];
+    int32_t ndim;
+    uint32_t volume;                 /* product of dims, < 2^31                 */
+    int32_t tile_leg;                /* leg with ostride == 1 for a tiled
+                                        transpose, -1 for a plain gather        */
+    int32_t pad;
+} FsPermEB;
+
+typedef struct FsPermTask {
+    int32_t eb;                      /* index into the EB table                 */
+    uint32_t start;                  /* first output-order position in the EB   */
+    uint32_t count;                  /* number of positions                     */
+    uint32_t pad;
+} FsPermTask;
+
+/*
+ * Replaces AbelianSymmetricTensor._permute_data -> _numba_abelian_transpose
+ * (frostspin/symmetric_tensor/abelian_symmetric_tensor.py:395-430, :103-250)
+ * for U(1) and Z2.  d_ebs / d_tasks are device tables built by the host plan
+ * (frostspin_b200/symmetric_tensor/abelian_plan.py).  in_len / out_len are the
+ * buffer lengths in elements; every EB is checked against them on the host
+ * side of the plan builder, and the kernel skips (and flags) any access that
+ * would fall outside, returning FS_ERR_BOUNDS after the stream synchronises
+ * when d_flag is not null.
+ */
+int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_out,
+                       int64_t out_len, const FsPermEB* d_ebs, int64_t n_ebs,
+                       const FsPermTask* d_tasks, int64_t n_tasks,
+                       int32_t* d_flag, void* stream);
+
+/* ------------------------------------------------------- grouped FP64 GEMM */
+/*
+ * One problem: C[MxN] = alpha * op(A) * op(B) + beta * C, all row-major with
+ * leading dimensions in elements.  transA == 0: A[i*lda + k]; transA == 1:
+ * A[k*lda + i].  transB == 0: B[k*ldb + j]; transB == 1: B[j*ldb + k].
+ * beta == 0 ignores the previous content of C (NaN-safe).
+ */
+typedef struct FsGemmProblem {
+    const double* A;
+    const double* B;
+    double* C;
+    int64_t lda, ldb, ldc;
+    int32_t M, N, K;
+    int32_t transA, transB;
+    int32_t pad;
+    double alpha, beta;
+} FsGemmProblem;
+
+typedef struct FsGemmTile {
+    int32_t problem;
+    int32_t tm;   /* tile row index    */
+    int32_t tn;   /* tile column index */
+    int32_t pad;
+} FsGemmTile;
+
+/* Output tile shape used by fs_grouped_dgemm (for building d_tiles). */
+int fs_dgemm_tile_shape(int32_t* tile_m, int32_t* tile_n);
+
+/*
+ * Replaces the per-irrep-block loop of SymmetricTensor.__matmul__
+ * (frostspin/symmetric_tensor/symmetric_tensor.py:453-489) and the sector
+ * products of construct_projectors (frostspin/ctmrg/ctm_renormalize.py:92-94,
+ * 122-123): every sector of one contraction in a single launch over a
+ * device tile list.
+ */
+int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_problems,
+                     const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
+
+/* -------------------------------------------------------------- block ops */
+/* x[0:n] *= alpha.  Replaces SymmetricTensor.__imul__/__itruediv__
+ * (symmetric_tensor.py:441-451) and scalar __mul__ (:377-424). */
+int fs_scale(double* d_x, int64_t n, double alpha, void* stream);
+
+/* y[0:n] = a*x + b*y.  Replaces the block sums of __add__/__sub__
+ * (symmetric_tensor.py:326-352). */
+int fs_axpby(const double* d_x, double* d_y, int64_t n, double a, double b,
+             void* stream);
+
+/*
+ * Weighted reductions over block lists.  A segment is a contiguous run of the
+ * buffer with a weight (the irrep dimension).
+ */
+typedef struct FsSegment {
+    int64_t offset;
+    int64_t length;
+    double weight;
+} FsSegment;
+
+/*
+ * out[0] = sum_s weight_s * sum_i x[offset_s + i]^2, the squared Frobenius
+ * norm SymmetricTensor.norm computes (symmetric_tensor.py:624-631) and
+ * DiagonalTensor.norm (diagonal_tensor.py:201-205).  d_partial is caller
+ * scratch of n_partial >= fs_reduce_partials() doubles.
+ */
+int fs_reduce_partials(void);
+int fs_weighted_sumsq(const double* d_x, const FsSegment* d_segs, int64_t n_segs,
+                      double* d_partial, int64_t n_partial, double* d_out,
+                      void* stream);
+
+/* out[0] = sum_s weight_s * sum_i x[offset_s + i]  (DiagonalTensor.sum,
+ * diagonal_tensor.py:195-199). Same scratch contract as fs_weighted_sumsq. */
+int fs_weighted_sum(const double* d_x, const FsSegment* d_segs, int64_t n_segs,
+                    double* d_partial, int64_t n_partial, double* d_out,
+                    void* stream);
+
+/*
+ * Pairwise block contraction: out[0] = sum_p weight_p * sum_{ij} A_p[i,j] B_p[j,i]
+ * (full_contract, symmetric_tensor.py:639-653) or, with b == NULL entries,
+ * sum_p weight_p * sum_i A_p[i,i] (trace, :633-637).  a_trans / b_trans mark
+ * F-order blocks.
+ */
+typedef struct FsPairBlock {
+    int64_t a_off, b_off;   /* b_off < 0: trace of A */
+    int32_t m, n;           /* logical shape of A_p  */
+    int32_t a_trans, b_trans;
+    double weight;
+} FsPairBlock;
+
+int fs_pair_contract(const double* d_a, const double* d_b,
+                     const FsPairBlock* d_pairs, int64_t n_pairs,
+                     double* d_partial, int64_t n_partial, double* d_out,
+                     void* stream);
+
+/*
+ * Diagonal scaling of blocks by 1-D weight vectors: out_b[i,j] = x_b[i,j] * d[j]
+ * (right) or d[i] (left).  Replaces SymmetricTensor._diagonal_mul
+ * (symmetric_tensor.py:1189-1248).  x may be F-order (x_trans); out is C-order.
+ */
+typedef struct FsDiagBlock {
+    int64_t x_off, out_off, d_off;
+    int32_t m, n;
+    int32_t x_trans, left;
+} FsDiagBlock;
+
+int fs_diag_mul(const double* d_x, const double* d_diag, double* d_out,
+                const FsDiagBlock* d_blocks, int64_t n_blocks, void* stream);
+
+/* Elementwise power of a weight vector, y = x^p, with p = -1, -0.5, 0.5 and
+ * 2 exact special cases (DiagonalTensor.__pow__, diagonal_tensor.py:133-143). */
+int fs_pow(const double* d_x, double* d_y, int64_t n, double p, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FROSTSPIN_B200_H */

@@ -1,0 +1,287 @@
+#!/usr/bin/env python
+"""Generate golden fixtures from the reference frostspin implementation.
+
+Run in a container where the reference tree is available (read-only):
+
+    PYTHONPATH=/root/reference python -O tests/golden/make_golden.py
+
+It imports frostspin 1.0.0 from that tree, builds seeded inputs, runs the
+reference's own operations and stores inputs and outputs as .npz files next to
+this script.  The fixtures are what pins the CPU oracle (oracle/) and, through
+it and directly, the device path.  Nothing at test time reads the reference.
+"""
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("FROSTSPIN_REFERENCE", "/root/reference")
+if REF not in sys.path:
+    sys.path.insert(0, REF)
+
+from frostspin import DiagonalTensor, U1SymmetricTensor  # noqa: E402
+from frostspin.misc_tools.svd_tools import find_block_cuts  # noqa: E402
+
+
+def pack_tensor(prefix, t, data):
+    """Store a reference SymmetricTensor with its own get_data_dic format."""
+    d = t.get_data_dic(prefix=prefix)
+    for k, v in d.items():
+        data[k] = np.asarray(v)
+
+
+def pack_diag(prefix, s, data):
+    for k, v in s.get_data_dic(prefix=prefix).items():
+        data[k] = np.asarray(v)
+
+
+def save(name, data):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **data)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def case_u1_reference_test():
+    """Shapes and signature of the reference's tests/test_u1_tensor.py:46-56."""
+    rng = np.random.default_rng(42)
+    c1 = np.array([-2, 0, 2], dtype=np.int8)
+    c2 = np.array([-3, -1, 1, 3], dtype=np.int8)
+    c3 = np.array([-2, -2, 0, 0, 0, 2, 2], dtype=np.int8)
+    c4 = np.array([-2, -1, 0, 1, 2], dtype=np.int8)
+    c5 = np.array([-3, -1, 0, 2], dtype=np.int8)
+    sig = np.array([1, 0, 0, 1, 1], dtype=bool)
+    t = U1SymmetricTensor.random((c1, c2), (c3, c4, c5), signature=sig, rng=rng)
+    data = {}
+    pack_tensor("in", t, data)
+    perms = [
+        ((3, 0, 2), (1, 4)),
+        ((3,), (1, 0, 4, 2)),
+        ((2, 3, 4), (0, 1)),
+        ((4, 1), (0, 3, 2)),
+        ((0, 1, 2, 3), (4,)),
+    ]
+    for i, (ra, ca) in enumerate(perms):
+        p = t.permute(ra, ca)
+        pack_tensor(f"perm{i}", p, data)
+        data[f"perm{i}_axes"] = np.array(ra + ca)
+        data[f"perm{i}_nrr"] = np.array(len(ra))
+        data[f"perm{i}_dense"] = p.toarray()
+    pack_tensor("transpose", t.transpose(), data)
+    pack_tensor("dagger", t.dagger(), data)
+    data["dense"] = t.toarray()
+    data["norm"] = np.array(t.norm())
+    data["full_contract_dagger"] = np.array(t.full_contract(t.dagger()))
+    # matmul: t (2 rows | 3 cols) @ t.dagger() (3 rows | 2 cols)
+    m = t @ t.dagger()
+    pack_tensor("matmul", m, data)
+    data["matmul_trace"] = np.array(m.trace())
+    # svd reconstruction and truncated svd spectra
+    u, s, v = t.svd()
+    pack_diag("svd_s", s, data)
+    ut, st, vt = t.truncated_svd(6)
+    pack_diag("tsvd_s", st, data)
+    pack_tensor("tsvd_usv", (ut * st) @ vt, data)
+    save("u1_reference_test", data)
+
+
+def z2_rep(pattern):
+    return np.array([-128 if c == "o" else 0 for c in pattern], dtype=np.int8)
+
+
+def case_z2_rank6():
+    """Z2 tensors with unsorted (interleaved) representations, rank 6."""
+    rng = np.random.default_rng(7)
+    reps = [z2_rep("eoeeo"), z2_rep("oe"), z2_rep("eeoo"), z2_rep("oeo"),
+            z2_rep("e"), z2_rep("oeeo")]
+    sig = np.array([0, 1, 1, 0, 1, 0], dtype=bool)
+    t = U1SymmetricTensor.random(tuple(reps[:3]), tuple(reps[3:]), signature=sig,
+                                 rng=rng)
+    data = {}
+    pack_tensor("in", t, data)
+    perms = [
+        ((0, 2, 4), (1, 3, 5)),
+        ((5, 1), (2, 0, 4, 3)),
+        ((3, 4, 5, 0, 1), (2,)),
+        ((2,), (5, 4, 3, 1, 0)),
+        ((1, 0, 3, 2), (5, 4)),
+    ]
+    for i, (ra, ca) in enumerate(perms):
+        p = t.permute(ra, ca)
+        pack_tensor(f"perm{i}", p, data)
+        data[f"perm{i}_axes"] = np.array(ra + ca)
+        data[f"perm{i}_nrr"] = np.array(len(ra))
+    save("z2_rank6", data)
+
+
+def microbench_rep(total, qmax):
+    """Charges -qmax..qmax with degeneracy ~ exp(-q^2/8), largest-remainder
+    rounding to `total`, sorted by charge."""
+    q = np.arange(-qmax, qmax + 1)
+    w = np.exp(-(q**2) / 8.0)
+    raw = w / w.sum() * total
+    deg = np.floor(raw).astype(int)
+    rem = total - deg.sum()
+    order = np.argsort(-(raw - deg), kind="stable")
+    deg[order[:rem]] += 1
+    return np.repeat(q, deg).astype(np.int8), deg
+
+
+def normal_tensor(cls, row_reps, col_reps, sig, rng):
+    irreps, shapes = cls.get_block_sizes(row_reps, col_reps, sig)
+    blocks = [rng.standard_normal(tuple(sh)) for sh in shapes]
+    return cls(row_reps, col_reps, blocks, irreps, sig)
+
+
+def case_u1_microbench_small():
+    """The U(1) microbench structure at reduced leg size (permute (0,2),(1,3)
+    then matmul against a tensor of the same structure)."""
+    rep, deg = microbench_rep(24, 4)
+    rng = np.random.default_rng(2024)
+    sig1 = np.array([False, False, True, True])
+    t1 = normal_tensor(U1SymmetricTensor, (rep, rep), (rep, rep), sig1, rng)
+    p = t1.permute((0, 2), (1, 3))
+    sig2 = np.array([True, False, False, True])
+    t2 = normal_tensor(U1SymmetricTensor, (rep, rep), (rep, rep), sig2, rng)
+    m = p @ t2
+    data = {"degen": deg}
+    pack_tensor("t1", t1, data)
+    pack_tensor("t2", t2, data)
+    pack_tensor("perm", p, data)
+    pack_tensor("matmul", m, data)
+    save("u1_microbench_small", data)
+    # full-size degeneracies of the benchmark legs (256 states, charges -4..4)
+    _, deg256 = microbench_rep(256, 4)
+    np.save(os.path.join(HERE, "u1_microbench_degen256.npy"), deg256)
+
+
+def case_find_block_cuts():
+    rng = np.random.default_rng(11)
+    data = {}
+    cases = []
+    for c in range(12):
+        nb = int(rng.integers(1, 7))
+        blocks = []
+        for _ in range(nb):
+            n = int(rng.integers(1, 30))
+            v = np.ascontiguousarray(np.sort(rng.random(n) ** 3)[::-1])
+            # plant quasi-degenerate multiplets
+            if n > 3:
+                v[1] = v[0] * (1 - 1e-6)
+                v[3] = v[2]
+            blocks.append(v)
+        if c % 3 == 0 and nb > 1:
+            blocks[1] = blocks[0].copy()
+        dims = rng.integers(1, 5, size=nb)
+        cut = int(rng.integers(1, 60))
+        degen = [1.0, 0.9999, 0.99][c % 3]
+        rtol = [None, 1e-3, 0.0][c % 3]
+        res = find_block_cuts(blocks, cut, dims=dims, rtol=rtol, degen_ratio=degen)
+        for i, b in enumerate(blocks):
+            data[f"c{c}_b{i}"] = b
+        data[f"c{c}_nb"] = np.array(nb)
+        data[f"c{c}_dims"] = dims
+        data[f"c{c}_cut"] = np.array(cut)
+        data[f"c{c}_degen"] = np.array(degen)
+        data[f"c{c}_rtol"] = np.array(np.nan if rtol is None else rtol)
+        data[f"c{c}_out"] = np.asarray(res)
+        cases.append(c)
+    data["ncases"] = np.array(len(cases))
+    save("find_block_cuts", data)
+
+
+def ising_reference_run(beta, chi, n_iter, seed, snapshots):
+    """examples/ising_classical_ctmrg.py Z2 part, restated with reference calls."""
+    import scipy.linalg as lg
+
+    sys.path.insert(0, os.path.join(REF, "..", "repo"))
+    D = 2
+    h = -2 * np.eye(2) + 1
+    sq_bw = lg.sqrtm(np.exp(-beta * h)).real
+    delta = np.zeros((D,) * 4)
+    delta[0, 0, 0, 0] = delta[1, 1, 1, 1] = 1
+    a0 = np.einsum("abcd,ai,bj,ck,dl->ijkl", delta, sq_bw, sq_bw, sq_bw, sq_bw)
+    mop = delta.copy()
+    mop[1, 1, 1, 1] = -1
+    mop = np.einsum("abcd,ai,bj,ck,dl->ijkl", mop, sq_bw, sq_bw, sq_bw, sq_bw)
+    K = np.array([[-1.0, 1.0], [1.0, 1.0]]) / np.sqrt(2)
+    a0d = np.einsum("abcd,ai,bj,ck,dl->ijkl", a0, K, K, K, K)
+    mopd = np.einsum("abcd,ai,bj,ck,dl->ijkl", mop, K, K, K, K)
+    rep = np.array([-128, 0], dtype=np.int8)
+    siga = np.array([False, False, True, True])
+    a = U1SymmetricTensor.from_array(a0d, (rep, rep), (rep, rep), signature=siga)
+    siga2 = np.array([False, True, True, True])
+    a2 = U1SymmetricTensor((rep, rep), (rep, rep), a.blocks, a.block_irreps, siga2)
+
+    rng = np.random.default_rng(seed)
+    d0o = d0e = chi // 2
+    s_odd = rng.normal(size=(d0o,))
+    s_odd = s_odd[np.abs(s_odd).argsort()[::-1]] / lg.norm(s_odd)
+    s_even = rng.normal(size=(d0e,))
+    s_even = s_even[np.abs(s_even).argsort()[::-1]] / lg.norm(s_even)
+    corner = np.array([-128] * d0o + [0] * d0e, dtype=np.int8)
+    s = DiagonalTensor((s_odd, s_even), corner, np.array([-128, 0], dtype=np.int8),
+                       [1, 1], "U1")
+    sigT = np.array([False, False, True])
+    T = U1SymmetricTensor.random((corner,), (rep, corner), signature=sigT, rng=rng)
+    temp = U1SymmetricTensor((corner,), (rep, corner), T.blocks, T.block_irreps,
+                             [1, 0, 0])
+    T = T + temp.permute((2,), (1, 0))
+    T /= T.norm()
+
+    def iterate(s, T):
+        Tp = T.permute((0, 1), (2,))
+        matC = Tp * s
+        matC = matC @ T
+        matC = matC.permute((1, 2), (0, 3))
+        matC = a2 @ matC
+        matC = matC.permute((0, 2), (1, 3))
+        news, U = matC.truncated_eigh(chi)
+        news /= news.norm()
+        newT = U.permute((1,), (0, 2))
+        newT = Tp @ newT
+        newT = newT.permute((1, 2), (0, 3))
+        newT = a @ newT
+        newT = newT.permute((0, 2), (1, 3))
+        newT = U.dagger() @ newT
+        newT /= newT.norm()
+        return news, newT
+
+    def energy(s, T):
+        Tp = T.permute((0, 1), (2,))
+        env = Tp * s
+        env = env @ env.permute((0,), (1, 2))
+        env = Tp @ env.permute((0,), (1, 2, 3))
+        left = env.permute((1, 2, 3), (0, 4))
+        right = env.permute((4, 0), (1, 2, 3))
+        env2 = (left @ right).toarray()
+        nr = np.einsum("abcdef,bgdc,afeg->", env2, a0d, a0d)
+        sdsr = np.einsum("abcdef,bgdc,afeg->", env2, mopd, mopd)
+        return -sdsr / nr
+
+    data = {"beta": np.array(beta), "chi": np.array(chi), "seed": np.array(seed)}
+    pack_diag("s0", s, data)
+    pack_tensor("T0", T, data)
+    for it in range(1, n_iter + 1):
+        s, T = iterate(s, T)
+        if it in snapshots:
+            pack_diag(f"s{it}", s, data)
+            pack_tensor(f"T{it}", T, data)
+            data[f"energy{it}"] = np.array(energy(s, T))
+    return data
+
+
+def case_ising():
+    data = ising_reference_run(0.44, 8, 10, 42, {1, 2, 3, 10})
+    save("ising_chi8", data)
+    data = ising_reference_run(0.44, 32, 100, 42, {1, 5, 100})
+    save("ising_chi32", data)
+
+
+if __name__ == "__main__":
+    case_u1_reference_test()
+    case_z2_rank6()
+    case_u1_microbench_small()
+    case_find_block_cuts()
+    case_ising()

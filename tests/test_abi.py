@@ -1,0 +1,126 @@
+"""The C-ABI library loads, exports every declared entry point, and its struct
+layouts match the numpy dtypes the host uses to build plan tables."""
+
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from frostspin_b200 import _native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER_DIR = os.path.join(ROOT, "include")
+
+
+def declared_functions():
+    names = []
+    for f in sorted(os.listdir(HEADER_DIR)):
+        if not f.endswith(".h"):
+            continue
+        text = open(os.path.join(HEADER_DIR, f)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(fs_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_library_loads_and_exports_all_symbols():
+    lib = _native.lib()
+    names = declared_functions()
+    assert len(names) >= 10
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _native.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_version_and_status_strings():
+    lib = _native.lib()
+    assert lib.fs_version() >= 10000
+    assert lib.fs_status_string(0) == b"ok"
+    assert lib.fs_status_string(-3).startswith(b"plan entry")
+
+
+def test_invalid_arguments_rejected_without_gpu_work():
+    # negative sizes are rejected on the host before any launch
+    lib = _native.lib()
+    assert lib.fs_scale(None, -1, 1.0, None) == -1
+    assert lib.fs_grouped_dgemm(None, 0, None, -5, None) == -1
+    assert lib.fs_abelian_permute(None, 0, None, 0, None, 0, None, -1, None, None) == -1
+    # zero work is a no-op success
+    assert lib.fs_scale(None, 0, 1.0, None) == 0
+
+
+LAYOUT_PROGRAM = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "frostspin_b200.h"
+#define F(T, f) printf("%s %s %zu\n", #T, #f, offsetof(T, f));
+#define S(T) printf("%s __size__ %zu\n", #T, sizeof(T));
+int main(void) {
+  S(FsPermEB) F(FsPermEB, obase) F(FsPermEB, nbase) F(FsPermEB, ostride)
+  F(FsPermEB, nstride) F(FsPermEB, dims) F(FsPermEB, divm) F(FsPermEB, divs)
+  F(FsPermEB, ndim) F(FsPermEB, volume) F(FsPermEB, tile_leg)
+  S(FsPermTask) F(FsPermTask, eb) F(FsPermTask, start) F(FsPermTask, count)
+  S(FsGemmProblem) F(FsGemmProblem, A) F(FsGemmProblem, B) F(FsGemmProblem, C)
+  F(FsGemmProblem, lda) F(FsGemmProblem, ldb) F(FsGemmProblem, ldc)
+  F(FsGemmProblem, M) F(FsGemmProblem, N) F(FsGemmProblem, K)
+  F(FsGemmProblem, transA) F(FsGemmProblem, transB)
+  F(FsGemmProblem, alpha) F(FsGemmProblem, beta)
+  S(FsGemmTile) F(FsGemmTile, problem) F(FsGemmTile, tm) F(FsGemmTile, tn)
+  S(FsSegment) F(FsSegment, offset) F(FsSegment, length) F(FsSegment, weight)
+  S(FsPairBlock) F(FsPairBlock, a_off) F(FsPairBlock, b_off) F(FsPairBlock, m)
+  F(FsPairBlock, n) F(FsPairBlock, a_trans) F(FsPairBlock, b_trans)
+  F(FsPairBlock, weight)
+  S(FsDiagBlock) F(FsDiagBlock, x_off) F(FsDiagBlock, out_off) F(FsDiagBlock, d_off)
+  F(FsDiagBlock, m) F(FsDiagBlock, n) F(FsDiagBlock, x_trans) F(FsDiagBlock, left)
+  return 0;
+}
+"""
+
+DTYPES = {
+    "FsPermEB": _native.PERM_EB_DTYPE,
+    "FsPermTask": _native.PERM_TASK_DTYPE,
+    "FsGemmProblem": _native.GEMM_PROBLEM_DTYPE,
+    "FsGemmTile": _native.GEMM_TILE_DTYPE,
+    "FsSegment": _native.SEGMENT_DTYPE,
+    "FsPairBlock": _native.PAIR_BLOCK_DTYPE,
+    "FsDiagBlock": _native.DIAG_BLOCK_DTYPE,
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    src = tmp_path / "layout.c"
+    exe = tmp_path / "layout"
+    src.write_text(LAYOUT_PROGRAM)
+    try:
+        subprocess.run(
+            ["gcc", "-std=c11", "-I", HEADER_DIR, str(src), "-o", str(exe)],
+            check=True, capture_output=True,
+        )
+    except FileNotFoundError:
+        pytest.skip("gcc not available")
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    seen = set()
+    for line in out.strip().splitlines():
+        struct, field, value = line.split()
+        dt = DTYPES[struct]
+        if field == "__size__":
+            assert dt.itemsize == int(value), struct
+        else:
+            assert dt.fields[field][1] == int(value), (struct, field)
+        seen.add(struct)
+    assert seen == set(DTYPES)
+
+
+def test_magic_division_exact():
+    from frostspin_b200.symmetric_tensor.abelian_plan import magic_divisor
+
+    rng = np.random.default_rng(0)
+    ds = np.concatenate([np.arange(1, 300), rng.integers(1, 2**31, 200)]).astype(np.uint64)
+    m, s = magic_divisor(ds)
+    ns = np.concatenate([np.arange(0, 5000), rng.integers(0, 2**32, 5000)]).astype(np.uint64)
+    for d, mm, ss in zip(ds, m.astype(np.uint64), s.astype(np.uint64), strict=True):
+        hi = (ns * mm) >> np.uint64(32)
+        q = (hi + ns) >> ss
+        assert np.array_equal(q, ns // d), int(d)
