@@ -290,7 +290,7 @@ def run_ours(args, world, rank, local):
 
     from frostspin_b200 import _native
 
-    wl = U1Microbench()
+    wl = U1Microbench(args.leg_states)
     t1, t2 = wl.device_inputs()
     m = wl.step(t1, t2)
     flops = wl.flops(t1.permute((0, 2), (1, 3)), t2)
@@ -460,6 +460,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["u1_microbench"], default="u1_microbench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--leg-states", type=int, default=LEG_STATES,
+                    help="states per leg (256 = the benchmark; smaller for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

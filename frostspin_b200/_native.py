@@ -61,6 +61,43 @@ GEMM_TILE_DTYPE = np.dtype(
     [("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")]
 )
 
+OZ_OPERAND_DTYPE = np.dtype(
+    [
+        ("src", "<u8"),
+        ("s_row", "<i8"),
+        ("s_k", "<i8"),
+        ("slices", "<u8"),
+        ("exps", "<u8"),
+        ("rows", "<i4"),
+        ("K", "<i4"),
+        ("rowtiles", "<i4"),
+        ("ktiles", "<i4"),
+    ]
+)
+
+OZ_PROBLEM_DTYPE = np.dtype(
+    [
+        ("a_slices", "<u8"),
+        ("b_slices", "<u8"),
+        ("a_exps", "<u8"),
+        ("b_exps", "<u8"),
+        ("C", "<u8"),
+        ("ldc", "<i8"),
+        ("M", "<i4"),
+        ("N", "<i4"),
+        ("K", "<i4"),
+        ("a_rowtiles", "<i4"),
+        ("b_rowtiles", "<i4"),
+        ("ktiles", "<i4"),
+        ("alpha", "<f8"),
+        ("beta", "<f8"),
+    ]
+)
+
+OZ_TILE_DTYPE = np.dtype([("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")])
+
+FS_OZAKI_MAX_SLICES = 8
+
 SEGMENT_DTYPE = np.dtype([("offset", "<i8"), ("length", "<i8"), ("weight", "<f8")])
 
 PAIR_BLOCK_DTYPE = np.dtype(
@@ -102,6 +139,9 @@ SIGNATURES = {
     ),
     "fs_dgemm_tile_shape": (ctypes.c_int, [_P, _P]),
     "fs_grouped_dgemm": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
+    "fs_ozaki_geometry": (ctypes.c_int, [_P, _P, _P, _P]),
+    "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
+    "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "fs_scale": (ctypes.c_int, [_P, _I64, _D, _P]),
     "fs_axpby": (ctypes.c_int, [_P, _P, _I64, _D, _D, _P]),
     "fs_pow": (ctypes.c_int, [_P, _P, _I64, _D, _P]),

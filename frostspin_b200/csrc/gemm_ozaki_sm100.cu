@@ -1,0 +1,523 @@
+// Grouped GEMM on the 5th-generation tensor cores (sm_100a, tcgen05) with
+// FP64-class accuracy: the Ozaki error-free splitting (Ozaki, Ogita, Oishi,
+// Rump, "Error-free transformations of matrix multiplication by using fast
+// routines of matrix multiplication", Numer. Algorithms 59, 2012), in the
+// integer form of Uchino, Ozaki and Imamura (2024): every row of A and every
+// column of B is scaled by a power of two into (-1, 1) and cut into S signed
+// 7-bit digits (int8 slices).  Products of slices are exact in int32, so
+//
+//   C = alpha * sum_{d=0}^{S-1} 2^(ea_i + eb_j - 7(d+2)) sum_{s+t=d} A_s B_t + beta * C
+//
+// is exact except for the dropped digits beyond S (relative error ~ 2^-7S of
+// the row/column maxima).  Each diagonal d is one int32 accumulation in TMEM
+// (tcgen05.mma kind::i8, M=128, N=256, K=32 per instruction), converted to
+// FP64 and added into C by the epilogue warps while the next diagonal
+// accumulates in the second TMEM buffer.
+//
+// The split kernels write the slices already in the 128-byte-swizzled K-major
+// tile layout the UMMA shared-memory descriptors expect, so every pipeline
+// stage is filled by two contiguous bulk copies (cp.async.bulk, the TMA unit)
+// without tensor maps.  All device waits are bounded: on timeout the kernel
+// raises FS_ERR_TIMEOUT in the caller's flag, drains its copies, frees TMEM
+// and returns.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace fsb {
+namespace oz {
+
+constexpr int kTileM = 128;       // rows of A per tile (UMMA M)
+constexpr int kTileN = 256;       // rows of B^T per tile (UMMA N)
+constexpr int kTileK = 128;       // int8 elements (bytes) per k-step = one swizzle atom
+constexpr int kStages = 4;
+constexpr int kABytes = kTileM * kTileK;            // 16 KB
+constexpr int kBBytes = kTileN * kTileK;            // 32 KB
+constexpr int kStageBytes = kABytes + kBBytes;      // 48 KB
+constexpr int kThreads = 192;                       // 6 warps
+constexpr int kTmemCols = 512;                      // two 256-column accumulators
+constexpr int kSplitRows = 128;                     // rows per slice tile
+constexpr long long kSpinLimit = 2000000000LL;      // ~1 s of clock64 at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false on timeout or when another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          volatile int* abort_flag) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > kSpinLimit) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Time-bounded wait that ignores the abort flag (used to drain in-flight work).
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kSpinLimit) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// K-major operand, 128-byte swizzle, 8-row core groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr & 0x3FFFF) >> 4);        // start address
+    d |= static_cast<uint64_t>(1) << 16;                      // leading byte offset (unused)
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;              // stride byte offset
+    d |= static_cast<uint64_t>(1) << 46;                      // descriptor version (sm_100)
+    d |= static_cast<uint64_t>(2) << 61;                      // SWIZZLE_128B
+    return d;
+}
+
+// kind::i8 instruction descriptor: S32 accumulate, signed A and B, K-major both.
+constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                            (static_cast<uint32_t>(kTileN >> 3) << 17) |
+                            (static_cast<uint32_t>(kTileM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+          "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+          "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// --------------------------------------------------------------- split kernels
+
+// exps[v] = e with max_k |x(v, k)| < 2^e (frexp exponent; 0 for a zero vector).
+// One warp per vector.
+__global__ void __launch_bounds__(256)
+    k_oz_exponents(const FsOzOperand* __restrict__ ops, int64_t n_ops) {
+    const int op_id = blockIdx.y;
+    if (op_id >= n_ops) return;
+    const FsOzOperand op = ops[op_id];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int64_t v = static_cast<int64_t>(blockIdx.x) * 8 + warp; v < op.rows;
+         v += static_cast<int64_t>(gridDim.x) * 8) {
+        double m = 0.0;
+        for (int64_t k = lane; k < op.K; k += 32)
+            m = fmax(m, fabs(__ldg(op.src + v * op.s_row + k * op.s_k)));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) {
+            int e = 0;
+            if (m > 0.0) frexp(m, &e);
+            op.exps[v] = e;
+        }
+    }
+}
+
+// Writes the S digit slices of one operand in swizzled tile layout:
+// tile (s, kt, rt) of 128 rows x 128 bytes at ((s * ktiles + kt) * rowtiles + rt) * 16 KB,
+// row r at r * 128 bytes, 16-byte chunk c stored at chunk (c ^ (r & 7)).
+__global__ void __launch_bounds__(1024)
+    k_oz_split(const FsOzOperand* __restrict__ ops, int64_t n_ops, int nslices) {
+    const int op_id = blockIdx.y;
+    if (op_id >= n_ops) return;
+    const FsOzOperand op = ops[op_id];
+    const int r = threadIdx.x / 8;      // row in tile
+    const int c = threadIdx.x % 8;      // 16-byte chunk (16 k values)
+    const int64_t ntiles = static_cast<int64_t>(op.rowtiles) * op.ktiles;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int kt = static_cast<int>(tile / op.rowtiles);
+        const int rt = static_cast<int>(tile % op.rowtiles);
+        const int64_t row = static_cast<int64_t>(rt) * kSplitRows + r;
+        const int64_t k0 = static_cast<int64_t>(kt) * kTileK + c * 16;
+        const int e = (row < op.rows) ? op.exps[row] : 0;
+        double x[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int64_t k = k0 + j;
+            x[j] = (row < op.rows && k < op.K)
+                       ? ldexp(__ldg(op.src + row * op.s_row + k * op.s_k), -e)
+                       : 0.0;
+        }
+        const int64_t slice_stride = static_cast<int64_t>(op.ktiles) * op.rowtiles * kABytes;
+        int8_t* dst = op.slices + (static_cast<int64_t>(kt) * op.rowtiles + rt) * kABytes +
+                      r * 128 + ((c ^ (r & 7)) * 16);
+        for (int s = 0; s < nslices; ++s) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const double t = x[j] * 128.0;
+                const double dgt = trunc(t);
+                x[j] = t - dgt;
+                const uint32_t byte = static_cast<uint32_t>(static_cast<int32_t>(dgt)) & 0xFFu;
+                w[j / 4] |= byte << (8 * (j % 4));
+            }
+            *reinterpret_cast<uint4*>(dst + s * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ GEMM kernel
+
+struct __align__(8) Barriers {
+    uint64_t full[kStages];
+    uint64_t empty[kStages];
+    uint64_t acc_full[2];
+    uint64_t acc_empty[2];
+    uint64_t mma_drain;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+// Iteration order shared by the producer and the MMA issuer: for every tile of
+// this CTA, for every diagonal d (S-1 down to 0), for every K chunk, for every
+// slice pair (s, d - s), for every k-tile of the chunk.
+struct PassIter {
+    int nslices, ktiles, chunk;
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_oz_gemm(const FsOzProblem* __restrict__ probs, int64_t n_probs,
+              const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
+              int chunk_ktiles, int32_t* flag) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* smem = smem_raw + (base - raw);
+    Barriers* bars = reinterpret_cast<Barriers*>(smem + kStages * kStageBytes);
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_addr(&bars->full[s]), 1);
+            mbar_init(smem_addr(&bars->empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_addr(&bars->acc_full[b]), 1);
+            mbar_init(smem_addr(&bars->acc_empty[b]), 4);
+        }
+        mbar_init(smem_addr(&bars->mma_drain), 1);
+        bars->abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(&bars->tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bars->tmem_base;
+    volatile int* abort_flag = &bars->abort_flag;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            uint32_t issued_mask = 0;          // stages with a copy issued
+            uint32_t issued_parity = 0;        // full-barrier parity of that copy
+            for (int64_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x) {
+                const FsOzTile tile = tiles[t];
+                const FsOzProblem p = probs[tile.problem];
+                const int64_t a_slice = static_cast<int64_t>(p.ktiles) * p.a_rowtiles * kABytes;
+                const int64_t b_slice = static_cast<int64_t>(p.ktiles) * p.b_rowtiles * kABytes;
+                for (int d = nslices - 1; ok && d >= 0; --d) {
+                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
+                        for (int s = 0; ok && s <= d; ++s) {
+                            const int tt = d - s;
+                            for (int kt = k0; kt < k1; ++kt) {
+                                if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1,
+                                               abort_flag)) {
+                                    ok = false;
+                                    break;
+                                }
+                                const uint32_t full = smem_addr(&bars->full[stage]);
+                                mbar_expect_tx(full, kStageBytes);
+                                const int8_t* a = p.a_slices + s * a_slice +
+                                                  (static_cast<int64_t>(kt) * p.a_rowtiles + tile.tm) * kABytes;
+                                const int8_t* b = p.b_slices + tt * b_slice +
+                                                  (static_cast<int64_t>(kt) * p.b_rowtiles + 2 * tile.tn) * kABytes;
+                                const uint32_t dst = base + stage * kStageBytes;
+                                bulk_g2s(dst, a, kABytes, full);
+                                bulk_g2s(dst + kABytes, b, kBBytes, full);
+                                issued_mask |= 1u << stage;
+                                issued_parity = (issued_parity & ~(1u << stage)) | (phase << stage);
+                                if (++stage == kStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            // drain: every issued copy must have landed before the CTA exits
+            for (int s = 0; s < kStages; ++s) {
+                if (issued_mask & (1u << s)) {
+                    if (!mbar_wait_drain(smem_addr(&bars->full[s]), (issued_parity >> s) & 1u))
+                        *abort_flag = 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool ok = true;
+            for (int64_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x) {
+                const FsOzTile tile = tiles[t];
+                const FsOzProblem p = probs[tile.problem];
+                for (int d = nslices - 1; ok && d >= 0; --d) {
+                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
+                        if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1,
+                                       abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t tmem_d = tmem_base + acc * kTileN;
+                        uint32_t accumulate = 0;
+                        for (int s = 0; ok && s <= d; ++s) {
+                            for (int kt = k0; kt < k1; ++kt) {
+                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
+                                    ok = false;
+                                    break;
+                                }
+                                tc_fence_after();
+                                const uint32_t a_addr = base + stage * kStageBytes;
+                                const uint32_t b_addr = a_addr + kABytes;
+#pragma unroll
+                                for (int k = 0; k < kTileK / 32; ++k) {
+                                    mma_i8(tmem_d, smem_desc_sw128(a_addr + 32 * k),
+                                           smem_desc_sw128(b_addr + 32 * k), accumulate);
+                                    accumulate = 1;
+                                }
+                                mma_commit(smem_addr(&bars->empty[stage]));
+                                if (++stage == kStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        }
+                        if (!ok) break;
+                        mma_commit(smem_addr(&bars->acc_full[acc]));
+                        if (++acc == 2) {
+                            acc = 0;
+                            acc_phase ^= 1;
+                        }
+                    }
+                }
+            }
+            // drain: all issued MMAs complete before TMEM is released
+            mma_commit(smem_addr(&bars->mma_drain));
+            if (!mbar_wait_drain(smem_addr(&bars->mma_drain), 0)) *abort_flag = 1;
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue
+        const int quad = warp % 4;           // TMEM lane quadrant this warp may read
+        const int row_in_tile = quad * 32 + lane;
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        bool ok = true;
+        for (int64_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x) {
+            const FsOzTile tile = tiles[t];
+            const FsOzProblem p = probs[tile.problem];
+            const int64_t row = static_cast<int64_t>(tile.tm) * kTileM + row_in_tile;
+            const int col0 = tile.tn * kTileN;
+            const bool row_ok = row < p.M;
+            const int ea = row_ok ? p.a_exps[row] : 0;
+            bool first = true;
+            for (int d = nslices - 1; ok && d >= 0; --d) {
+                for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                    // one lane waits, the warp follows its verdict, so the
+                    // warp-wide tcgen05.ld below is never reached by a subset
+                    int got = 0;
+                    if (lane == 0)
+                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag)
+                                  ? 1
+                                  : 0;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (!got) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) +
+                                           acc * kTileN;
+                    const int shift = -7 * (d + 2);
+                    for (int cb = 0; cb < kTileN; cb += 16) {
+                        uint32_t v[16];
+                        tmem_ld16(taddr + cb, v);
+                        if (!row_ok) continue;
+                        double* crow = p.C + row * p.ldc;
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const int col = col0 + cb + j;
+                            if (col >= p.N) continue;
+                            const double val =
+                                p.alpha * ldexp(static_cast<double>(static_cast<int32_t>(v[j])),
+                                                ea + p.b_exps[col] + shift);
+                            if (first) {
+                                crow[col] = (p.beta == 0.0) ? val : fma(p.beta, crow[col], val);
+                            } else {
+                                crow[col] += val;
+                            }
+                        }
+                    }
+                    first = false;
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_addr(&bars->acc_empty[acc]));
+                    if (++acc == 2) {
+                        acc = 0;
+                        acc_phase ^= 1;
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) raise_flag(flag, FS_ERR_TIMEOUT);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+}  // namespace oz
+}  // namespace fsb
+
+extern "C" int fs_ozaki_geometry(int32_t* tile_m, int32_t* tile_n, int32_t* tile_k,
+                                 int32_t* split_rows) {
+    if (!tile_m || !tile_n || !tile_k || !split_rows) return FS_ERR_INVALID_ARG;
+    *tile_m = fsb::oz::kTileM;
+    *tile_n = fsb::oz::kTileN;
+    *tile_k = fsb::oz::kTileK;
+    *split_rows = fsb::oz::kSplitRows;
+    return FS_OK;
+}
+
+extern "C" int fs_ozaki_split(const FsOzOperand* d_ops, int64_t n_ops, int32_t max_rows,
+                              int32_t max_tiles, int32_t nslices, void* stream) {
+    if (n_ops < 0 || max_rows < 0 || max_tiles < 0) return FS_ERR_INVALID_ARG;
+    if (nslices < 1 || nslices > FS_OZAKI_MAX_SLICES) return FS_ERR_INVALID_ARG;
+    if (n_ops == 0 || max_tiles == 0) return FS_OK;
+    if (d_ops == nullptr) return FS_ERR_INVALID_ARG;
+    if (n_ops > 65535) return FS_ERR_TOO_LARGE;
+    cudaStream_t s = fsb::as_stream(stream);
+    const int gx = static_cast<int>(
+        ((max_rows + 7) / 8) < 4 * fsb::kNumSM ? ((max_rows + 7) / 8) : 4 * fsb::kNumSM);
+    fsb::oz::k_oz_exponents<<<dim3(gx > 0 ? gx : 1, static_cast<unsigned>(n_ops)), 256, 0, s>>>(
+        d_ops, n_ops);
+    int st = fsb::launch_status();
+    if (st != FS_OK) return st;
+    const int tx = max_tiles < 4 * fsb::kNumSM ? max_tiles : 4 * fsb::kNumSM;
+    fsb::oz::k_oz_split<<<dim3(tx, static_cast<unsigned>(n_ops)), 1024, 0, s>>>(d_ops, n_ops,
+                                                                                nslices);
+    return fsb::launch_status();
+}
+
+extern "C" int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
+                             const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
+                             int32_t chunk_ktiles, int32_t* d_flag, void* stream) {
+    if (n_probs < 0 || n_tiles < 0 || chunk_ktiles < 1) return FS_ERR_INVALID_ARG;
+    if (nslices < 1 || nslices > FS_OZAKI_MAX_SLICES) return FS_ERR_INVALID_ARG;
+    if (n_tiles == 0) return FS_OK;
+    if (d_probs == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    // int32 accumulation bound: nslices * chunk * 128 * 127^2 < 2^31
+    const long long bound = static_cast<long long>(nslices) * chunk_ktiles * fsb::oz::kTileK *
+                            127LL * 127LL;
+    if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
+    const int smem = fsb::oz::kStages * fsb::oz::kStageBytes +
+                     static_cast<int>(sizeof(fsb::oz::Barriers)) + 1024;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fsb::oz::k_oz_gemm,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) {
+            fsb::set_last_cuda_error(e);
+            return FS_ERR_CUDA;
+        }
+        configured = true;
+    }
+    const int grid = static_cast<int>(n_tiles < fsb::kNumSM ? n_tiles : fsb::kNumSM);
+    fsb::oz::k_oz_gemm<<<grid, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
+        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
+    return fsb::launch_status();
+}

@@ -16,7 +16,7 @@ from . import device as dev
 # ----------------------------------------------------------------- precision
 
 _PRECISION = {"gemm": "fp64"}
-PRECISIONS = ("fp64",)
+PRECISIONS = ("fp64",) + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
 
 
 def gemm_precision():
@@ -24,7 +24,10 @@ def gemm_precision():
 
 
 def set_gemm_precision(mode):
-    """Select the sector-GEMM arithmetic: "fp64" (plain double precision)."""
+    """Select the sector-GEMM arithmetic: "fp64" (plain double precision on the
+    FP64 pipes) or "ozakiS" (FP64 operands split into S int8 digit slices, exact
+    int32 products on the tcgen05 tensor cores, FP64 recombination; relative
+    error ~2^-7S of the row/column maxima, S = 3..8)."""
     if mode not in PRECISIONS:
         msg = f"unknown GEMM precision {mode!r}; choose from {PRECISIONS}"
         raise ValueError(msg)
@@ -81,10 +84,13 @@ def grouped_gemm(problems):
         arr["alpha"][i] = p.get("alpha", 1.0)
         arr["beta"][i] = p.get("beta", 0.0)
         ntile.append(((M + tm - 1) // tm) * ((N + tn - 1) // tn))
-    if gemm_precision() == "fp64":
+    mode = gemm_precision()
+    if mode == "fp64":
         _dgemm(arr, problems, tm, tn, np.array(ntile, dtype=np.int64))
+    elif mode.startswith("ozaki"):
+        ozaki_gemm(arr, int(mode[5:]))
     else:  # pragma: no cover - guarded by set_gemm_precision
-        raise ValueError(gemm_precision())
+        raise ValueError(mode)
 
 
 def _tile_table(arr, tm, tn, ntile):
@@ -115,6 +121,131 @@ def _dgemm(arr, problems, tm, tn, ntile):
         dev.stream(),
     )
     return d_prob, d_tiles
+
+
+# ------------------------------------------------- tcgen05 (Ozaki int8) GEMM
+
+OZ_TILE_M = 128
+OZ_TILE_N = 256
+OZ_TILE_K = 128
+OZ_SPLIT_ROWS = 128
+OZ_TILE_BYTES = OZ_SPLIT_ROWS * OZ_TILE_K
+
+
+def ozaki_chunk_ktiles(nslices):
+    """Largest number of k-tiles whose int32 diagonal sums cannot overflow."""
+    return max(1, (2**31 - 1) // (nslices * OZ_TILE_K * 127 * 127))
+
+
+def _round_up(x, a):
+    return (x + a - 1) // a * a
+
+
+def ozaki_plan(arr, nslices):
+    """Operand/problem/tile tables and workspace layout for a problem array
+    (GEMM_PROBLEM_DTYPE).  Returns (ops, probs, tiles, workspace_bytes, offsets)
+    with pointer fields relative to the workspace base (patched on launch)."""
+    n = arr.size
+    ops = np.zeros(2 * n, dtype=_native.OZ_OPERAND_DTYPE)
+    probs = np.zeros(n, dtype=_native.OZ_PROBLEM_DTYPE)
+    off = 0
+    rel = {"a_slices": [], "b_slices": [], "a_exps": [], "b_exps": []}
+    tiles = []
+    for i in range(n):
+        M, N, K = int(arr["M"][i]), int(arr["N"][i]), int(arr["K"][i])
+        kt = max(1, (K + OZ_TILE_K - 1) // OZ_TILE_K)
+        art = (M + OZ_SPLIT_ROWS - 1) // OZ_SPLIT_ROWS
+        brt = 2 * ((N + OZ_TILE_N - 1) // OZ_TILE_N)
+        a_bytes = nslices * kt * art * OZ_TILE_BYTES
+        b_bytes = nslices * kt * brt * OZ_TILE_BYTES
+        a_sl, off = off, off + a_bytes
+        b_sl, off = off, off + b_bytes
+        a_ex, off = off, off + _round_up(4 * max(M, 1), 256)
+        b_ex, off = off, off + _round_up(4 * max(N, 1), 256)
+        off = _round_up(off, 1024)
+        lda, ldb = int(arr["lda"][i]), int(arr["ldb"][i])
+        ta, tb = int(arr["transA"][i]), int(arr["transB"][i])
+        # operand A: element (i, k) of op(A)
+        ops[2 * i] = (arr["A"][i], 1 if ta else lda, lda if ta else 1, a_sl, a_ex, M, K, art, kt)
+        # operand B^T: element (j, k) = op(B)[k, j]
+        ops[2 * i + 1] = (arr["B"][i], ldb if tb else 1, 1 if tb else ldb, b_sl, b_ex, N, K, brt, kt)
+        probs[i] = (a_sl, b_sl, a_ex, b_ex, arr["C"][i], arr["ldc"][i], M, N, K, art, brt, kt,
+                    arr["alpha"][i], arr["beta"][i])
+        for tm_ in range(art):
+            for tn_ in range((N + OZ_TILE_N - 1) // OZ_TILE_N):
+                tiles.append((i, tm_, tn_, 0, K))
+        rel["a_slices"].append(a_sl)
+    tile_arr = np.zeros(len(tiles), dtype=_native.OZ_TILE_DTYPE)
+    if tiles:
+        t = np.array(tiles, dtype=np.int64)
+        order = np.argsort(-t[:, 4], kind="stable")
+        t = t[order]
+        tile_arr["problem"] = t[:, 0]
+        tile_arr["tm"] = t[:, 1]
+        tile_arr["tn"] = t[:, 2]
+    return ops, probs, tile_arr, off
+
+
+def ozaki_gemm(arr, nslices, workspace=None):
+    """Run the problems of `arr` (GEMM_PROBLEM_DTYPE) on the tcgen05 Ozaki path.
+    The workspace is a caller-owned uint8 device buffer (allocated here from
+    torch's caching allocator when not given)."""
+    ops, probs, tiles, nbytes = ozaki_plan(arr, nslices)
+    if tiles.size == 0:
+        return
+    if workspace is None or workspace.numel() < nbytes:
+        workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev.device())
+    base = workspace.data_ptr()
+    for f in ("slices", "exps"):
+        ops[f] += np.uint64(base)
+    for f in ("a_slices", "b_slices", "a_exps", "b_exps"):
+        probs[f] += np.uint64(base)
+    d_ops = dev.upload(ops)
+    d_probs = dev.upload(probs)
+    d_tiles = dev.upload(tiles)
+    max_rows = int(ops["rows"].max())
+    max_tiles = int((ops["rowtiles"].astype(np.int64) * ops["ktiles"]).max())
+    for start in range(0, ops.size, 65534):
+        sub = slice(start, min(ops.size, start + 65534))
+        _native.call(
+            "fs_ozaki_split",
+            d_ops.data_ptr() + start * ops.itemsize,
+            ops[sub].size,
+            max_rows,
+            max_tiles,
+            nslices,
+            dev.stream(),
+        )
+    flag = torch.zeros(1, dtype=torch.int32, device=dev.device())
+    _native.call(
+        "fs_ozaki_gemm",
+        d_probs.data_ptr(),
+        probs.size,
+        d_tiles.data_ptr(),
+        tiles.size,
+        nslices,
+        ozaki_chunk_ktiles(nslices),
+        flag.data_ptr(),
+        dev.stream(),
+    )
+    _OZ_FLAGS.append(flag)
+    if len(_OZ_FLAGS) > 64:
+        check_ozaki_flags()
+    return workspace
+
+
+_OZ_FLAGS = []
+
+
+def check_ozaki_flags():
+    """Synchronise on the error flags of past tcgen05 launches; raise if a bounded
+    device wait ran out."""
+    flags = list(_OZ_FLAGS)
+    _OZ_FLAGS.clear()
+    for f in flags:
+        v = int(f.item())
+        if v != 0:
+            _native.check(v, "fs_ozaki_gemm (device flag)")
 
 
 # --------------------------------------------------------------- reductions

@@ -312,7 +312,7 @@ def build_abelian_permute_plan(
     plan.offsets = new_offsets
     plan.size = total
     plan.ebs = ebs
-    plan.tasks = _make_tasks(vol)
+    plan.tasks = _make_tasks(ebs)
     plan.in_len = int(in_len)
     plan.device_tables = None
     return plan
@@ -379,17 +379,26 @@ def _pack_ebs(dims, ostride, nstride, obase, nbase, present):
     return out, vol
 
 
-def _make_tasks(vol, chunk=TASK_CHUNK):
-    nchunk = (vol + chunk - 1) // chunk
+def _make_tasks(ebs, chunk=TASK_CHUNK):
+    """Split every EB into tasks of whole rows (runs along the last leg) holding
+    about `chunk` entries each."""
+    n_eb = ebs.size
+    if n_eb == 0:
+        return np.zeros(0, dtype=PERM_TASK_DTYPE)
+    r = ebs["ndim"].astype(np.int64)
+    inner = ebs["dims"][np.arange(n_eb), r - 1].astype(np.int64)
+    rows = ebs["volume"].astype(np.int64) // inner
+    per = np.maximum(1, chunk // inner)
+    nchunk = (rows + per - 1) // per
     n = int(nchunk.sum())
     tasks = np.zeros(n, dtype=PERM_TASK_DTYPE)
-    eb = np.repeat(np.arange(vol.size), nchunk)
+    eb = np.repeat(np.arange(n_eb), nchunk)
     first = np.repeat(np.cumsum(nchunk) - nchunk, nchunk)
     k = np.arange(n) - first
-    start = k * chunk
+    start = k * per[eb]
     tasks["eb"] = eb
     tasks["start"] = start
-    tasks["count"] = np.minimum(chunk, vol[eb] - start)
+    tasks["count"] = np.minimum(per[eb], rows[eb] - start)
     return tasks
 
 

@@ -26,7 +26,7 @@ def relayout_blocks(data, offsets, shapes, trans, new_offsets, total):
     present = np.ones(nb, dtype=bool)
     ebs, vol = _pack_ebs(dims, ostride, nstride, np.asarray(offsets, dtype=np.int64),
                          np.asarray(new_offsets, dtype=np.int64), present)
-    tasks = _make_tasks(vol)
+    tasks = _make_tasks(ebs)
     d_ebs = dev.upload(ebs)
     d_tasks = dev.upload(tasks)
     _native.call(

@@ -51,7 +51,8 @@ const char* fs_last_cuda_error(void);
  * one EB the input and output element offsets are affine in the per-leg local
  * indices, so the whole permutation is a batch of strided copies.  Legs are
  * listed outer to inner in output order; dims[ndim-1] is the output-innermost
- * leg.  divm/divs are the Granlund-Montgomery magic multiplier and shift for
+ * leg; a row is one run along it, and tasks cover whole rows.
+ * divm/divs are the Granlund-Montgomery magic multiplier and shift for
  * dividing by dims[k] (host computed).  obase < 0 marks an EB whose source
  * block is absent: its output entries are written as zeros.
  */
@@ -74,8 +75,8 @@ typedef struct FsPermEB {
 
 typedef struct FsPermTask {
     int32_t eb;                      /* index into the EB table                 */
-    uint32_t start;                  /* first output-order position in the EB   */
-    uint32_t count;                  /* number of positions                     */
+    uint32_t start;                  /* first row (run along the last leg)      */
+    uint32_t count;                  /* number of rows                          */
     uint32_t pad;
 } FsPermTask;
 
@@ -131,6 +132,70 @@ int fs_dgemm_tile_shape(int32_t* tile_m, int32_t* tile_n);
  */
 int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_problems,
                      const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
+
+/* ------------------------------------- grouped GEMM on tcgen05 (Ozaki int8) */
+/*
+ * FP64-class GEMM on the int8 tensor cores (tcgen05.mma kind::i8): every row of
+ * op(A) and column of op(B) is scaled by a power of two into (-1, 1) and cut
+ * into nslices signed 7-bit digits; diagonal sums of slice products are exact
+ * int32 accumulations in TMEM, recombined in FP64.  Relative error per entry is
+ * ~2^(-7 nslices) of the product of the row/column maxima.
+ *
+ * Workspace (caller-owned device memory, computed by the host): per operand
+ * nslices * ktiles * rowtiles tiles of 128 rows x 128 bytes, written by
+ * fs_ozaki_split in the 128-byte-swizzled K-major layout, plus one int32
+ * exponent per row.  B operands are stored transposed (rows = columns of op(B))
+ * and their rowtiles must be even (256-row MMA tiles).
+ */
+#define FS_OZAKI_MAX_SLICES 8
+
+typedef struct FsOzOperand {
+    const double* src;     /* element (row, k) at src[row*s_row + k*s_k]      */
+    int64_t s_row, s_k;
+    int8_t* slices;        /* workspace, nslices*ktiles*rowtiles*16384 bytes */
+    int32_t* exps;         /* workspace, rows entries                          */
+    int32_t rows, K;
+    int32_t rowtiles, ktiles;
+} FsOzOperand;
+
+typedef struct FsOzProblem {
+    const int8_t* a_slices;
+    const int8_t* b_slices;
+    const int32_t* a_exps;
+    const int32_t* b_exps;
+    double* C;             /* row-major M x N, leading dimension ldc          */
+    int64_t ldc;
+    int32_t M, N, K;
+    int32_t a_rowtiles, b_rowtiles, ktiles;
+    double alpha, beta;
+} FsOzProblem;
+
+typedef struct FsOzTile {
+    int32_t problem;
+    int32_t tm;            /* 128-row tile index of C                         */
+    int32_t tn;            /* 256-column tile index of C                      */
+    int32_t pad;
+} FsOzTile;
+
+/* Tile geometry of the tcgen05 kernel (M tile, N tile, K bytes per stage,
+ * rows per slice tile). */
+int fs_ozaki_geometry(int32_t* tile_m, int32_t* tile_n, int32_t* tile_k,
+                      int32_t* split_rows);
+
+/* Exponents and digit slices of every operand (grid.y = operand, <= 65535). */
+int fs_ozaki_split(const FsOzOperand* d_ops, int64_t n_ops, int32_t max_rows,
+                   int32_t max_tiles, int32_t nslices, void* stream);
+
+/*
+ * The mixed-precision replacement of fs_grouped_dgemm for the same call sites
+ * (symmetric_tensor.py:453-489, ctm_renormalize.py:92-94, 122-123).
+ * chunk_ktiles bounds the k-tiles accumulated in int32 before conversion:
+ * nslices * chunk_ktiles * 128 * 127^2 must stay below 2^31.  A bounded wait
+ * that runs out writes FS_ERR_TIMEOUT to d_flag (if not null).
+ */
+int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
+                  const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
+                  int32_t chunk_ktiles, int32_t* d_flag, void* stream);
 
 /* -------------------------------------------------------------- block ops */
 /* x[0:n] *= alpha.  Replaces SymmetricTensor.__imul__/__itruediv__

@@ -74,6 +74,14 @@ int main(void) {
   F(FsPairBlock, weight)
   S(FsDiagBlock) F(FsDiagBlock, x_off) F(FsDiagBlock, out_off) F(FsDiagBlock, d_off)
   F(FsDiagBlock, m) F(FsDiagBlock, n) F(FsDiagBlock, x_trans) F(FsDiagBlock, left)
+  S(FsOzOperand) F(FsOzOperand, src) F(FsOzOperand, s_row) F(FsOzOperand, s_k)
+  F(FsOzOperand, slices) F(FsOzOperand, exps) F(FsOzOperand, rows) F(FsOzOperand, K)
+  F(FsOzOperand, rowtiles) F(FsOzOperand, ktiles)
+  S(FsOzProblem) F(FsOzProblem, a_slices) F(FsOzProblem, b_slices) F(FsOzProblem, a_exps)
+  F(FsOzProblem, b_exps) F(FsOzProblem, C) F(FsOzProblem, ldc) F(FsOzProblem, M)
+  F(FsOzProblem, N) F(FsOzProblem, K) F(FsOzProblem, a_rowtiles) F(FsOzProblem, b_rowtiles)
+  F(FsOzProblem, ktiles) F(FsOzProblem, alpha) F(FsOzProblem, beta)
+  S(FsOzTile) F(FsOzTile, problem) F(FsOzTile, tm) F(FsOzTile, tn)
   return 0;
 }
 """
@@ -86,6 +94,9 @@ DTYPES = {
     "FsSegment": _native.SEGMENT_DTYPE,
     "FsPairBlock": _native.PAIR_BLOCK_DTYPE,
     "FsDiagBlock": _native.DIAG_BLOCK_DTYPE,
+    "FsOzOperand": _native.OZ_OPERAND_DTYPE,
+    "FsOzProblem": _native.OZ_PROBLEM_DTYPE,
+    "FsOzTile": _native.OZ_TILE_DTYPE,
 }
 
 

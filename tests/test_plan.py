@@ -125,3 +125,22 @@ def test_plan_random_tensors(seed):
         axes = tuple(int(a) for a in rng.permutation(ndim))
         new_nrr = int(rng.integers(1, ndim))
         check_against_oracle(t, axes, new_nrr, trans=bool(seed % 4 == 1), rng=rng)
+
+
+def test_task_tables_cover_every_row_once():
+    from frostspin_b200.symmetric_tensor.abelian_plan import _make_tasks
+
+    d = load("u1_microbench_small")
+    t1 = oracle_from_dic(d, "t1")
+    plan, _ = run_plan(t1, (0, 2, 1, 3), 2)
+    for chunk in (1, 7, 64, 8192):
+        tasks = _make_tasks(plan.ebs, chunk)
+        r = plan.ebs["ndim"].astype(np.int64)
+        inner = plan.ebs["dims"][np.arange(plan.ebs.size), r - 1].astype(np.int64)
+        rows = plan.ebs["volume"].astype(np.int64) // inner
+        covered = np.zeros(plan.ebs.size, dtype=np.int64)
+        for t in tasks:
+            assert t["start"] == covered[t["eb"]]
+            assert t["count"] >= 1
+            covered[t["eb"]] += t["count"]
+        assert np.array_equal(covered, rows)
