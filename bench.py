@@ -196,6 +196,17 @@ def measure_dgemm_peak():
     return best
 
 
+def tensor_ops_ozaki(p, t2, S):
+    """int8 tensor-core operations the Ozaki path issues: S(S+1)/2 slice products
+    of 2 M N K each on the padded tile grid (128 x 256 x 128)."""
+    common, i1, i2 = np.intersect1d(p.block_irreps, t2.block_irreps, return_indices=True)
+    m = p.block_shapes[i1, 0]
+    k = p.block_shapes[i1, 1]
+    n = t2.block_shapes[i2, 1]
+    pad = lambda x, a: (x + a - 1) // a * a  # noqa: E731
+    return float((2 * pad(m, 128) * pad(n, 256) * pad(k, 128)).sum() * S * (S + 1) // 2)
+
+
 # --------------------------------------------------------------- CPU baseline
 
 
@@ -290,6 +301,9 @@ def run_ours(args, world, rank, local):
 
     from frostspin_b200 import _native
 
+    from frostspin_b200 import linalg
+
+    linalg.set_gemm_precision(args.precision)
     wl = U1Microbench(args.leg_states)
     t1, t2 = wl.device_inputs()
     m = wl.step(t1, t2)
@@ -314,8 +328,25 @@ def run_ours(args, world, rank, local):
     clk = clocks.stop()
     barrier(world)
     elapsed = max_over_ranks(start.elapsed_time(end) * 1e-3, world)
-    perm_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    perm_ms_in_step = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
     gemm_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+
+    # the permute kernel timed alone (inside the step it runs at the clocks the
+    # power-capped GEMM leaves it)
+    for _ in range(3):
+        t1.permute((0, 2), (1, 3))
+    pclk = ClockSampler(local)
+    pclk.start()
+    ps = torch.cuda.Event(enable_timing=True)
+    pe = torch.cuda.Event(enable_timing=True)
+    n_perm = 20
+    ps.record()
+    for _ in range(n_perm):
+        t1.permute((0, 2), (1, 3))
+    pe.record()
+    torch.cuda.synchronize()
+    perm_clk = pclk.stop()
+    perm_ms = ps.elapsed_time(pe) / n_perm
 
     # end-to-end through the public API from pinned host buffers
     rep = wl.rep
@@ -338,12 +369,40 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_elapsed = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
 
-    hbm, _bf16, peak_kind = load_peaks()
+    hbm, bf16, peak_kind = load_peaks()
     fp64_peak = measure_dgemm_peak()
+    linalg.check_ozaki_flags()
     perm_bytes = 16.0 * wl.ncoeff
     perm_gbs = perm_bytes / (perm_ms * 1e-3) / 1e9
     gemm_tf = flops / (gemm_ms * 1e-3) / 1e12
     value = world * args.steps / elapsed
+    if args.precision.startswith("ozaki"):
+        S = int(args.precision[5:])
+        int8_ops = tensor_ops_ozaki(t1.permute((0, 2), (1, 3)), t2, S)
+        int8_peak = 2.0 * bf16
+        gemm_roofline = {
+            "bound": "tensor",
+            "kernel": "k_oz_gemm",
+            "achieved": int8_ops / (gemm_ms * 1e-3) / 1e12,
+            "peak": int8_peak,
+            "unit": "TOP/s (int8)",
+            "frac": int8_ops / (gemm_ms * 1e-3) / 1e12 / int8_peak,
+            "peak_kind": f"2 x {peak_kind} bf16 dense (int8 dense rate is twice bf16)",
+            "traffic": None,
+            "int8_ops_per_step": int8_ops,
+            "note": "ms includes the digit-split kernels",
+        }
+    else:
+        gemm_roofline = {
+            "bound": "tensor",
+            "kernel": "k_grouped_dgemm",
+            "achieved": gemm_tf,
+            "peak": fp64_peak,
+            "unit": "TFLOP/s",
+            "frac": gemm_tf / fp64_peak,
+            "peak_kind": "measured in-run cuBLAS DGEMM 8192^3 (no FP64 figure in the peaks file)",
+            "traffic": None,
+        }
     line = {
         "metric": "U(1) microbench permute+grouped-matmul steps/s",
         "value": value,
@@ -363,20 +422,12 @@ def run_ours(args, world, rank, local):
             "legs": "4 x 256 states, U(1) charges -4..4, degeneracies [7,17,32,46,52,46,32,17,7]",
             "ncoeff": wl.ncoeff,
             "gemm_flop_per_step": flops,
-            "gemm_precision": "fp64",
+            "gemm_precision": args.precision,
             "l2": "inputs 3.64 GB per tensor > 126 MB L2; no flush needed",
             "parallelism": f"replicas x{world}",
         },
-        "roofline": {
-            "bound": "tensor",
-            "kernel": "k_grouped_dgemm",
-            "achieved": gemm_tf,
-            "peak": fp64_peak,
-            "unit": "TFLOP/s",
-            "frac": gemm_tf / fp64_peak,
-            "peak_kind": "measured in-run cuBLAS DGEMM 8192^3 (no FP64 figure in the peaks file)",
-            "traffic": None,
-        },
+        "roofline": gemm_roofline,
+        "gemm_vs_cublas_dgemm": gemm_tf / fp64_peak,
         "roofline_permute": {
             "bound": "hbm",
             "kernel": "k_perm_gather",
@@ -384,8 +435,11 @@ def run_ours(args, world, rank, local):
             "peak": hbm,
             "unit": "GB/s",
             "frac": perm_gbs / hbm,
-            "peak_kind": f"{peak_kind} copy bandwidth",
+            "peak_kind": f"{peak_kind} copy bandwidth (burst)",
             "ms": perm_ms,
+            "timing": "20 back-to-back launches timed alone with CUDA events",
+            "ms_inside_step": perm_ms_in_step,
+            "clocks": perm_clk,
         },
         "e2e": {
             "value": world * e2e_steps / e2e_elapsed,
@@ -393,7 +447,7 @@ def run_ours(args, world, rank, local):
             "h2d_bytes_per_step": int(h1.numel() * 8 + h2.numel() * 8),
             "d2h_bytes_per_step": int(t1.data.numel() * 8),
         },
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (2 if args.precision == "fp64" else 4) * args.steps,
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -460,6 +514,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["u1_microbench"], default="u1_microbench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64",
+                    help="sector GEMM arithmetic: fp64 or ozakiS (S = 3..8 int8 slices)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
                     help="states per leg (256 = the benchmark; smaller for profiling)")
     args = ap.parse_args()

@@ -6,34 +6,42 @@
 // plan splits the tensor into elementary blocks (one irrep segment per leg), in
 // which both the source and destination offsets are affine in the leg indices.
 // Legs are ordered by output stride, so the last leg is the output-innermost
-// one.  A *row* of an elementary block is one run along that leg; the kernel
-// decodes the outer multi-index once per row (Granlund-Montgomery division with
-// host-computed constants, descriptor in shared memory) and copies the run with
-// a lane group sized to it, so stores are coalesced along the output and, when
-// the source keeps the same innermost leg, loads are too.  Absent source blocks
-// produce zeros, as the reference's zero-initialised output blocks do.
+// one; positions are decoded with Granlund-Montgomery division by the leg
+// sizes (host-computed constants).  Absent source blocks produce zeros, as the
+// reference's zero-initialised output blocks do.
 #include "common.cuh"
 
 namespace fsb {
 
 constexpr int kPermThreads = 256;
-constexpr int kPermInnerUnroll = 4;
+constexpr int kPermUnroll = 4;
+constexpr int kPermMaxRows = 1024;   // rows per task (shared-memory row table)
 
+// One task = a range of rows of one elementary block, a row being one run along
+// the output-innermost leg (length L).  Phase 1 decodes the outer multi-index
+// of every row of the task once (Granlund-Montgomery division by the leg sizes)
+// into a shared-memory table of source/destination row offsets, checking both
+// ends of each row against the buffers.  Phase 2 walks the task's entries flat:
+// entry idx -> (row, i) by one division by L, offsets from the table plus i
+// times the innermost strides.  Consecutive threads write consecutive outputs
+// (coalesced stores) and read consecutive inputs whenever the source keeps the
+// same innermost leg; each thread keeps kPermUnroll loads in flight.
 __global__ void __launch_bounds__(kPermThreads, 4)
-    k_perm_rows(const double* __restrict__ in, int64_t in_len, double* __restrict__ out,
-                int64_t out_len, const FsPermEB* __restrict__ ebs, int64_t n_ebs,
-                const FsPermTask* __restrict__ tasks, int64_t n_tasks, int32_t* flag) {
+    k_perm_gather(const double* __restrict__ in, int64_t in_len, double* __restrict__ out,
+                  int64_t out_len, const FsPermEB* __restrict__ ebs, int64_t n_ebs,
+                  const FsPermTask* __restrict__ tasks, int64_t n_tasks, int32_t* flag) {
     __shared__ FsPermEB e;
+    __shared__ int64_t row_src[kPermMaxRows];
+    __shared__ int64_t row_dst[kPermMaxRows];
     static_assert(sizeof(FsPermEB) % 8 == 0, "descriptor must be 8-byte granular");
     constexpr int kWords = sizeof(FsPermEB) / 8;
-    const int lane = threadIdx.x % 32;
     for (int64_t t = blockIdx.x; t < n_tasks; t += gridDim.x) {
         const FsPermTask task = tasks[t];
-        if (task.eb < 0 || task.eb >= n_ebs) {
+        __syncthreads();  // previous task done with the shared tables
+        if (task.eb < 0 || task.eb >= n_ebs || task.count > kPermMaxRows) {
             if (threadIdx.x == 0) raise_flag(flag, FS_ERR_BOUNDS);
             continue;
         }
-        __syncthreads();
         if (threadIdx.x < kWords) {
             reinterpret_cast<int64_t*>(&e)[threadIdx.x] =
                 reinterpret_cast<const int64_t*>(ebs + task.eb)[threadIdx.x];
@@ -48,14 +56,9 @@ __global__ void __launch_bounds__(kPermThreads, 4)
         const int64_t osL = e.ostride[nd - 1];
         const int64_t nsL = e.nstride[nd - 1];
         const bool zero_fill = e.obase < 0;
-        // lane group: smallest power of two >= L, at most a warp
-        const int g = (L >= 32) ? 32 : (L <= 1 ? 1 : (1 << (32 - __clz(L - 1))));
-        const int lg = lane % g;
-        const int grp = static_cast<int>(threadIdx.x) / g;
-        const int ngrp = kPermThreads / g;
-        const uint32_t end = task.start + task.count;
-        for (uint32_t row = task.start + grp; row < end; row += ngrp) {
-            uint32_t q = row;
+        const int nrows = static_cast<int>(task.count);
+        for (int j = threadIdx.x; j < nrows; j += kPermThreads) {
+            uint32_t q = task.start + static_cast<uint32_t>(j);
             int64_t so = e.obase, dof = e.nbase;
             for (int k = nd - 2; k >= 0; --k) {
                 const uint32_t qq = fast_div(q, e.divm[k], e.divs[k]);
@@ -64,36 +67,41 @@ __global__ void __launch_bounds__(kPermThreads, 4)
                 so += static_cast<int64_t>(i) * e.ostride[k];
                 dof += static_cast<int64_t>(i) * e.nstride[k];
             }
-            for (uint32_t i0 = lg; i0 < L; i0 += g * kPermInnerUnroll) {
-                double v[kPermInnerUnroll];
-                int64_t dst[kPermInnerUnroll];
+            const int64_t dlast = dof + static_cast<int64_t>(L - 1) * nsL;
+            const int64_t slast = so + static_cast<int64_t>(L - 1) * osL;
+            bool ok = dof >= 0 && dlast < out_len;
+            if (!zero_fill) ok = ok && so >= 0 && slast < in_len;
+            if (!ok) {
+                raise_flag(flag, FS_ERR_BOUNDS);
+                dof = -1;
+            }
+            row_src[j] = so;
+            row_dst[j] = dof;
+        }
+        __syncthreads();
+        const uint32_t total = static_cast<uint32_t>(nrows) * L;
+        const uint32_t mL = e.divm[nd - 1], sL = e.divs[nd - 1];
+        for (uint32_t i0 = threadIdx.x; i0 < total; i0 += kPermThreads * kPermUnroll) {
+            double v[kPermUnroll];
+            int64_t dst[kPermUnroll];
 #pragma unroll
-                for (int u = 0; u < kPermInnerUnroll; ++u) {
-                    const uint32_t i = i0 + u * g;
-                    dst[u] = -1;
-                    v[u] = 0.0;
-                    if (i < L) {
-                        const int64_t d = dof + static_cast<int64_t>(i) * nsL;
-                        if (d < 0 || d >= out_len) {
-                            raise_flag(flag, FS_ERR_BOUNDS);
-                            continue;
-                        }
-                        dst[u] = d;
-                        if (!zero_fill) {
-                            const int64_t s = so + static_cast<int64_t>(i) * osL;
-                            if (s >= 0 && s < in_len) {
-                                v[u] = __ldg(in + s);
-                            } else {
-                                raise_flag(flag, FS_ERR_BOUNDS);
-                                dst[u] = -1;
-                            }
-                        }
+            for (int u = 0; u < kPermUnroll; ++u) {
+                const uint32_t idx = i0 + u * kPermThreads;
+                dst[u] = -1;
+                v[u] = 0.0;
+                if (idx < total) {
+                    const uint32_t row = fast_div(idx, mL, sL);
+                    const uint32_t i = idx - row * L;
+                    const int64_t rd = row_dst[row];
+                    if (rd >= 0) {
+                        dst[u] = rd + static_cast<int64_t>(i) * nsL;
+                        if (!zero_fill) v[u] = __ldg(in + row_src[row] + static_cast<int64_t>(i) * osL);
                     }
                 }
+            }
 #pragma unroll
-                for (int u = 0; u < kPermInnerUnroll; ++u) {
-                    if (dst[u] >= 0) out[dst[u]] = v[u];
-                }
+            for (int u = 0; u < kPermUnroll; ++u) {
+                if (dst[u] >= 0) out[dst[u]] = v[u];
             }
         }
     }
@@ -109,9 +117,10 @@ extern "C" int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_
     if (n_tasks == 0) return FS_OK;
     if (d_out == nullptr || d_ebs == nullptr || d_tasks == nullptr) return FS_ERR_INVALID_ARG;
     if (d_in == nullptr && in_len > 0) return FS_ERR_INVALID_ARG;
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 8;
+    // one wave of resident CTAs (4 per SM at the kernel's register budget)
+    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 4;
     const int grid = static_cast<int>(n_tasks < max_grid ? n_tasks : max_grid);
-    fsb::k_perm_rows<<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
+    fsb::k_perm_gather<<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
         d_in, in_len, d_out, out_len, d_ebs, n_ebs, d_tasks, n_tasks, d_flag);
     return fsb::launch_status();
 }

@@ -379,23 +379,25 @@ def _pack_ebs(dims, ostride, nstride, obase, nbase, present):
     return out, vol
 
 
+MAX_TASK_ROWS = 1024
+
+
 def _make_tasks(ebs, chunk=TASK_CHUNK):
-    """Split every EB into tasks of whole rows (runs along the last leg) holding
-    about `chunk` entries each."""
+    """Split every EB into tasks of whole rows (runs along the last leg): about
+    `chunk` entries and at most MAX_TASK_ROWS rows per task."""
     n_eb = ebs.size
     if n_eb == 0:
         return np.zeros(0, dtype=PERM_TASK_DTYPE)
     r = ebs["ndim"].astype(np.int64)
     inner = ebs["dims"][np.arange(n_eb), r - 1].astype(np.int64)
     rows = ebs["volume"].astype(np.int64) // inner
-    per = np.maximum(1, chunk // inner)
+    per = np.clip(chunk // inner, 1, MAX_TASK_ROWS)
     nchunk = (rows + per - 1) // per
     n = int(nchunk.sum())
     tasks = np.zeros(n, dtype=PERM_TASK_DTYPE)
     eb = np.repeat(np.arange(n_eb), nchunk)
     first = np.repeat(np.cumsum(nchunk) - nchunk, nchunk)
-    k = np.arange(n) - first
-    start = k * per[eb]
+    start = (np.arange(n) - first) * per[eb]
     tasks["eb"] = eb
     tasks["start"] = start
     tasks["count"] = np.minimum(per[eb], rows[eb] - start)

@@ -51,7 +51,8 @@ const char* fs_last_cuda_error(void);
  * one EB the input and output element offsets are affine in the per-leg local
  * indices, so the whole permutation is a batch of strided copies.  Legs are
  * listed outer to inner in output order; dims[ndim-1] is the output-innermost
- * leg; a row is one run along it, and tasks cover whole rows.
+ * leg; a row is one run along it, and a task covers at most 1024 whole rows
+ * of one EB.
  * divm/divs are the Granlund-Montgomery magic multiplier and shift for
  * dividing by dims[k] (host computed).  obase < 0 marks an EB whose source
  * block is absent: its output entries are written as zeros.
@@ -76,7 +77,7 @@ typedef struct FsPermEB {
 typedef struct FsPermTask {
     int32_t eb;                      /* index into the EB table                 */
     uint32_t start;                  /* first row (run along the last leg)      */
-    uint32_t count;                  /* number of rows                          */
+    uint32_t count;                  /* number of rows, at most 1024            */
     uint32_t pad;
 } FsPermTask;
 
@@ -196,6 +197,7 @@ int fs_ozaki_split(const FsOzOperand* d_ops, int64_t n_ops, int32_t max_rows,
 int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
                   const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
                   int32_t chunk_ktiles, int32_t* d_flag, void* stream);
+
 
 /* -------------------------------------------------------------- block ops */
 /* x[0:n] *= alpha.  Replaces SymmetricTensor.__imul__/__itruediv__

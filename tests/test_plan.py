@@ -128,19 +128,19 @@ def test_plan_random_tensors(seed):
 
 
 def test_task_tables_cover_every_row_once():
-    from frostspin_b200.symmetric_tensor.abelian_plan import _make_tasks
+    from frostspin_b200.symmetric_tensor.abelian_plan import MAX_TASK_ROWS, _make_tasks
 
     d = load("u1_microbench_small")
     t1 = oracle_from_dic(d, "t1")
     plan, _ = run_plan(t1, (0, 2, 1, 3), 2)
-    for chunk in (1, 7, 64, 8192):
+    r = plan.ebs["ndim"].astype(np.int64)
+    inner = plan.ebs["dims"][np.arange(plan.ebs.size), r - 1].astype(np.int64)
+    rows = plan.ebs["volume"].astype(np.int64) // inner
+    for chunk in (1, 7, 64, 8192, 10**7):
         tasks = _make_tasks(plan.ebs, chunk)
-        r = plan.ebs["ndim"].astype(np.int64)
-        inner = plan.ebs["dims"][np.arange(plan.ebs.size), r - 1].astype(np.int64)
-        rows = plan.ebs["volume"].astype(np.int64) // inner
         covered = np.zeros(plan.ebs.size, dtype=np.int64)
         for t in tasks:
             assert t["start"] == covered[t["eb"]]
-            assert t["count"] >= 1
+            assert 1 <= t["count"] <= MAX_TASK_ROWS
             covered[t["eb"]] += t["count"]
         assert np.array_equal(covered, rows)
