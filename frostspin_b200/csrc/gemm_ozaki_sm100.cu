@@ -22,6 +22,12 @@
 // and returns.
 #include <math.h>
 
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 
 namespace fsb {
@@ -520,4 +526,166 @@ extern "C" int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
     fsb::oz::k_oz_gemm<<<grid, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
         d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
     return fsb::launch_status();
+}
+
+// ------------------------------------------------------ no-allocation variant
+//
+// Some callers cannot allocate device memory: a host application whose own
+// memory pool has already reserved the device (a cudaMalloc from a library
+// inside it would fail or fragment that pool), or a C / Fortran driver with no
+// device allocator of its own that only holds the input and output buffers.
+// fs_ozaki_gemm_noalloc serves them: the digit slices, exponents and launch
+// tables live in one fixed file-scope device array instead of a caller-provided
+// workspace.  Every GPU that loads this library holds that array until the
+// process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(48) << 20;   // 48 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+std::mutex g_noalloc_mutex;
+uint8_t* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+static __device__ __align__(256) uint8_t g_ozaki_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+// Device address of the scratch array on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device with that device current.
+int noalloc_scratch(uint8_t** base) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        fsb::set_last_cuda_error(e);
+        return FS_ERR_CUDA;
+    }
+    if (device < 0 || device >= kNoAllocMaxDevices) return FS_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_base[device] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_ozaki_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            fsb::set_last_cuda_error(e);
+            return FS_ERR_CUDA;
+        }
+        g_noalloc_base[device] = static_cast<uint8_t*>(p);
+    }
+    *base = g_noalloc_base[device];
+    return FS_OK;
+}
+
+int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+extern "C" int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_problems,
+                                     int32_t nslices, void* stream) {
+    using namespace fsb::oz;
+    if (n_problems < 0 || nslices < 1 || nslices > FS_OZAKI_MAX_SLICES)
+        return FS_ERR_INVALID_ARG;
+    if (n_problems == 0) return FS_OK;
+    if (h_problems == nullptr) return FS_ERR_INVALID_ARG;
+
+    // layout of the scratch: per problem slices and exponents, then the tables
+    std::vector<FsOzOperand> ops;
+    std::vector<FsOzProblem> probs;
+    std::vector<std::pair<int32_t, FsOzTile>> tiles;  // (K, tile) for ordering
+    int64_t off = 0;
+    int32_t max_rows = 0, max_tiles = 0;
+    for (int64_t i = 0; i < n_problems; ++i) {
+        const FsGemmProblem& g = h_problems[i];
+        if (g.M < 0 || g.N < 0 || g.K < 0) return FS_ERR_INVALID_ARG;
+        if (g.M == 0 || g.N == 0) continue;
+        if (g.C == nullptr || (g.K > 0 && (g.A == nullptr || g.B == nullptr)))
+            return FS_ERR_INVALID_ARG;
+        const int32_t kt = g.K > 0 ? (g.K + kTileK - 1) / kTileK : 1;
+        const int32_t art = (g.M + kSplitRows - 1) / kSplitRows;
+        const int32_t ntn = (g.N + kTileN - 1) / kTileN;
+        const int32_t brt = 2 * ntn;
+        const int64_t a_sl = off;
+        off += static_cast<int64_t>(nslices) * kt * art * kABytes;
+        const int64_t b_sl = off;
+        off += static_cast<int64_t>(nslices) * kt * brt * kABytes;
+        const int64_t a_ex = off;
+        off += round_up(4 * static_cast<int64_t>(g.M), 256);
+        const int64_t b_ex = off;
+        off += round_up(4 * static_cast<int64_t>(g.N), 256);
+        off = round_up(off, 1024);
+        if (off > static_cast<int64_t>(kNoAllocScratchBytes)) return FS_ERR_TOO_LARGE;
+        // offsets are patched to device addresses once the layout is known
+        FsOzOperand a{g.A, g.transA ? 1 : g.lda, g.transA ? g.lda : 1,
+                      reinterpret_cast<int8_t*>(a_sl), reinterpret_cast<int32_t*>(a_ex),
+                      g.M, g.K, art, kt};
+        FsOzOperand b{g.B, g.transB ? g.ldb : 1, g.transB ? 1 : g.ldb,
+                      reinterpret_cast<int8_t*>(b_sl), reinterpret_cast<int32_t*>(b_ex),
+                      g.N, g.K, brt, kt};
+        ops.push_back(a);
+        ops.push_back(b);
+        FsOzProblem p{reinterpret_cast<const int8_t*>(a_sl), reinterpret_cast<const int8_t*>(b_sl),
+                      reinterpret_cast<const int32_t*>(a_ex), reinterpret_cast<const int32_t*>(b_ex),
+                      g.C, g.ldc, g.M, g.N, g.K, art, brt, kt, g.alpha, g.beta};
+        const int32_t pid = static_cast<int32_t>(probs.size());
+        probs.push_back(p);
+        for (int32_t tm = 0; tm < art; ++tm)
+            for (int32_t tn = 0; tn < ntn; ++tn) tiles.push_back({g.K, FsOzTile{pid, tm, tn, 0}});
+        max_rows = std::max(max_rows, std::max(g.M, g.N));
+        max_tiles = std::max(max_tiles, std::max(art, brt) * kt);
+    }
+    if (tiles.empty()) return FS_OK;
+    std::stable_sort(tiles.begin(), tiles.end(),
+                     [](const auto& x, const auto& y) { return x.first > y.first; });
+
+    const int64_t ops_off = off;
+    const int64_t probs_off = round_up(ops_off + static_cast<int64_t>(ops.size() * sizeof(FsOzOperand)), 256);
+    const int64_t tiles_off = round_up(probs_off + static_cast<int64_t>(probs.size() * sizeof(FsOzProblem)), 256);
+    const int64_t end = tiles_off + static_cast<int64_t>(tiles.size() * sizeof(FsOzTile));
+    if (end > static_cast<int64_t>(kNoAllocScratchBytes)) return FS_ERR_TOO_LARGE;
+
+    uint8_t* base = nullptr;
+    int st = noalloc_scratch(&base);
+    if (st != FS_OK) return st;
+    const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+    for (auto& o : ops) {
+        o.slices = reinterpret_cast<int8_t*>(b + reinterpret_cast<uintptr_t>(o.slices));
+        o.exps = reinterpret_cast<int32_t*>(b + reinterpret_cast<uintptr_t>(o.exps));
+    }
+    for (auto& p : probs) {
+        p.a_slices = reinterpret_cast<const int8_t*>(b + reinterpret_cast<uintptr_t>(p.a_slices));
+        p.b_slices = reinterpret_cast<const int8_t*>(b + reinterpret_cast<uintptr_t>(p.b_slices));
+        p.a_exps = reinterpret_cast<const int32_t*>(b + reinterpret_cast<uintptr_t>(p.a_exps));
+        p.b_exps = reinterpret_cast<const int32_t*>(b + reinterpret_cast<uintptr_t>(p.b_exps));
+    }
+    std::vector<uint8_t> staging(static_cast<size_t>(end - ops_off), 0);
+    std::memcpy(staging.data(), ops.data(), ops.size() * sizeof(FsOzOperand));
+    std::memcpy(staging.data() + (probs_off - ops_off), probs.data(),
+                probs.size() * sizeof(FsOzProblem));
+    FsOzTile* tdst = reinterpret_cast<FsOzTile*>(staging.data() + (tiles_off - ops_off));
+    for (size_t i = 0; i < tiles.size(); ++i) tdst[i] = tiles[i].second;
+
+    cudaStream_t s = fsb::as_stream(stream);
+    // pageable source: the call returns once the bytes are staged, so the
+    // host vectors may go out of scope afterwards
+    cudaError_t e = cudaMemcpyAsync(base + ops_off, staging.data(), staging.size(),
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        fsb::set_last_cuda_error(e);
+        return FS_ERR_CUDA;
+    }
+    const FsOzOperand* d_ops = reinterpret_cast<const FsOzOperand*>(base + ops_off);
+    const int64_t n_ops = static_cast<int64_t>(ops.size());
+    for (int64_t start = 0; start < n_ops; start += 65534) {
+        const int64_t cnt = std::min<int64_t>(65534, n_ops - start);
+        st = fs_ozaki_split(d_ops + start, cnt, max_rows, max_tiles, nslices, stream);
+        if (st != FS_OK) return st;
+    }
+    const int32_t chunk = static_cast<int32_t>(std::max<long long>(
+        1, ((1LL << 31) - 1) / (static_cast<long long>(nslices) * kTileK * 127 * 127)));
+    return fs_ozaki_gemm(reinterpret_cast<const FsOzProblem*>(base + probs_off),
+                         static_cast<int64_t>(probs.size()),
+                         reinterpret_cast<const FsOzTile*>(base + tiles_off),
+                         static_cast<int64_t>(tiles.size()), nslices, chunk, nullptr, stream);
 }

@@ -198,6 +198,31 @@ int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
                   const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
                   int32_t chunk_ktiles, int32_t* d_flag, void* stream);
 
+/*
+ * Grouped Ozaki GEMM that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: a host application whose own
+ * pool already reserved the device (a cudaMalloc from a library inside it
+ * would fail or fragment that pool), or a C / Fortran driver without a device
+ * allocator that only holds its input and output buffers.  The caller passes
+ * the problems as a HOST array of FsGemmProblem (same meaning as for
+ * fs_grouped_dgemm; A, B and C are device pointers).  Digit slices, exponents
+ * and launch tables go to a fixed 48 MiB file-scope device array inside this
+ * library, which every GPU that loads the library holds until the process
+ * exits; requests that do not fit return FS_ERR_TOO_LARGE before any GPU work
+ * (one 1024^3 product with 7 slices needs about 15 MiB).
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  The call
+ * copies its launch tables from host memory with cudaMemcpyAsync and calls no
+ * cudaMalloc, cudaFree or allocating library routine.  All calls on a device
+ * share that device's array and every call rewrites what it reads, so calls
+ * that overlap on the GPU (for example on two streams of the same device) race;
+ * serialise them.  A bounded device wait that runs out ends the kernel early but
+ * is not reported through this entry point.
+ */
+int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_problems,
+                          int32_t nslices, void* stream);
 
 /* -------------------------------------------------------------- block ops */
 /* x[0:n] *= alpha.  Replaces SymmetricTensor.__imul__/__itruediv__
