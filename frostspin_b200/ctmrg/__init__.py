@@ -6,8 +6,12 @@ from .classical_c4v import (
     ising_site_tensors,
     iterate_c4v,
 )
+from .ctm_environment import CTMEnvironment
+from .sequential_ctmrg import SequentialCTMRG
 
 __all__ = [
+    "CTMEnvironment",
+    "SequentialCTMRG",
     "energy_per_bond",
     "env_1site",
     "env_2sites",

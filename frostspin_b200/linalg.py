@@ -75,8 +75,8 @@ def grouped_gemm(problems):
         arr["A"][i] = p["A"].data_ptr() + 8 * int(p["a_off"])
         arr["B"][i] = p["B"].data_ptr() + 8 * int(p["b_off"])
         arr["C"][i] = p["C"].data_ptr() + 8 * int(p["c_off"])
-        arr["lda"][i] = M if p["a_trans"] else K
-        arr["ldb"][i] = K if p["b_trans"] else N
+        arr["lda"][i] = p.get("lda", M if p["a_trans"] else K)
+        arr["ldb"][i] = p.get("ldb", K if p["b_trans"] else N)
         arr["ldc"][i] = N
         arr["M"][i], arr["N"][i], arr["K"][i] = M, N, K
         arr["transA"][i] = int(bool(p["a_trans"]))
@@ -121,6 +121,56 @@ def _dgemm(arr, problems, tm, tn, ntile):
         dev.stream(),
     )
     return d_prob, d_tiles
+
+
+def _operand(t):
+    """(buffer, element offset, trans, leading dim) of a 2-D torch view whose
+    rows or columns are unit-stride; other views are made contiguous."""
+    if t.dim() != 2:
+        raise ValueError("block operands must be 2-D")
+    m, n = t.shape
+    s0, s1 = t.stride()
+    if s1 == 1 and (s0 >= n or m <= 1):
+        return t, max(s0, n), False
+    if s0 == 1 and (s1 >= m or n <= 1):
+        return t, max(s1, m), True
+    t = t.contiguous()
+    return t, n, False
+
+
+def matmul_blocks(lefts, rights, *, alpha=1.0):
+    """C_i = alpha * lefts[i] @ rights[i] for lists of 2-D device views, all in
+    one grouped GEMM launch; returns (buffer, offsets, shapes, views)."""
+    n = len(lefts)
+    shapes = np.array([(a.shape[0], b.shape[1]) for a, b in zip(lefts, rights, strict=True)],
+                      dtype=np.int64).reshape(-1, 2)
+    sizes = shapes[:, 0] * shapes[:, 1]
+    offsets = np.zeros(n, dtype=np.int64)
+    if n > 1:
+        offsets[1:] = np.cumsum(sizes[:-1])
+    out = dev.empty_f64(int(sizes.sum()))
+    problems = []
+    keep = []
+    for i, (a, b) in enumerate(zip(lefts, rights, strict=True)):
+        if a.shape[1] != b.shape[0]:
+            raise ValueError("inner dimensions do not match")
+        ta, lda, a_t = _operand(a)
+        tb, ldb, b_t = _operand(b)
+        keep += [ta, tb]
+        problems.append({
+            "A": ta, "a_off": 0, "a_trans": a_t, "lda": lda,
+            "B": tb, "b_off": 0, "b_trans": b_t, "ldb": ldb,
+            "C": out, "c_off": offsets[i], "M": a.shape[0], "N": b.shape[1],
+            "K": a.shape[1], "alpha": alpha,
+        })
+    for p in problems:
+        # data_ptr() of a view already includes its storage offset
+        p["a_off"] = 0
+        p["b_off"] = 0
+    if problems:
+        grouped_gemm(problems)
+    views = [out[o : o + m * k].view(m, k) for o, (m, k) in zip(offsets, shapes, strict=True)]
+    return out, offsets, shapes, views
 
 
 # ------------------------------------------------- tcgen05 (Ozaki int8) GEMM

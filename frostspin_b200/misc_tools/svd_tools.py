@@ -7,6 +7,42 @@ order.
 """
 
 import numpy as np
+import torch
+
+
+def truncated_svd_block(m, k, *, full, n_iter=6, oversampling=None):
+    """Leading singular triplets of one device block.
+
+    full=True: dense SVD (cuSOLVER), all values, like the reference's robust_svd
+    path (svd_tools.py:116-151).  Otherwise the k leading triplets by subspace
+    iteration with re-orthogonalisation (Halko, Martinsson, Tropp 2011,
+    Algorithm 4.4) on a basis of k + oversampling vectors -- the role ARPACK on
+    X^H X plays in the reference's sparse_svd (svd_tools.py:154-197), with the
+    products on the device.  Returns (U, s, Vh) with s decreasing.
+    """
+    nr, nc = m.shape
+    dmin = min(nr, nc)
+    if full or k >= dmin // 2:
+        u, s, vh = torch.linalg.svd(m, full_matrices=False)
+        return u, s, vh
+    from .. import linalg
+
+    p = k + 10 if oversampling is None else oversampling
+    kk = min(dmin, k + p)
+    g = torch.Generator(device=m.device)
+    g.manual_seed(1234 + nr * 7 + nc)
+    omega = torch.randn(nc, kk, dtype=m.dtype, device=m.device, generator=g)
+    _, _, _, (y,) = linalg.matmul_blocks([m], [omega])
+    q, _ = torch.linalg.qr(y, mode="reduced")
+    for _ in range(n_iter):
+        _, _, _, (z,) = linalg.matmul_blocks([m.T], [q])
+        z, _ = torch.linalg.qr(z, mode="reduced")
+        _, _, _, (y,) = linalg.matmul_blocks([m], [z])
+        q, _ = torch.linalg.qr(y, mode="reduced")
+    _, _, _, (b,) = linalg.matmul_blocks([q.T], [m])
+    ub, s, vh = torch.linalg.svd(b, full_matrices=False)
+    _, _, _, (u,) = linalg.matmul_blocks([q], [ub])
+    return u[:, :k], s[:k], vh[:k]
 
 
 def find_block_cuts(block_values, cut_target, *, dims=None, atol=0.0, rtol=None,

@@ -195,7 +195,6 @@ def ising_reference_run(beta, chi, n_iter, seed, snapshots):
     """examples/ising_classical_ctmrg.py Z2 part, restated with reference calls."""
     import scipy.linalg as lg
 
-    sys.path.insert(0, os.path.join(REF, "..", "repo"))
     D = 2
     h = -2 * np.eye(2) + 1
     sq_bw = lg.sqrtm(np.exp(-beta * h)).real
@@ -279,9 +278,47 @@ def case_ising():
     save("ising_chi32", data)
 
 
+def case_ctmrg_u1():
+    """SequentialCTMRG on the random U(1) AB/BA network of the reference's
+    tests/test_ctmrg.py:57-80 (distinct representation on every bond)."""
+    from frostspin.ctmrg import SequentialCTMRG
+
+    rng = np.random.default_rng(42)
+    rp = np.array([1, -1], dtype=np.int8)
+    ra = np.array([1, -1, 2], dtype=np.int8)
+    ru = np.array([1, 1, -1, 0, 2, -2], dtype=np.int8)
+    rr = np.array([2, 0, 1, -1, 0, 1, -1], dtype=np.int8)
+    rd = np.array([1, 1, -1, -2], dtype=np.int8)
+    rl = np.array([1, -2, 1, 0, 0], dtype=np.int8)
+    sA = np.array([False, False, True, True, True, True])
+    sB = np.array([False, False, False, False, False, False])
+    reps_A = (rp, ra, ru, rr, rd, rl)
+    reps_B = (rp, ra, rd, rl, ru, rr)
+    A = U1SymmetricTensor.random(reps_A[:2], reps_A[2:], rng=rng, signature=sA)
+    B = U1SymmetricTensor.random(reps_B[:2], reps_B[2:], rng=rng, signature=sB)
+    data = {}
+    pack_tensor("A", A, data)
+    pack_tensor("B", B, data)
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", (A, B), 20)
+    for it in range(4):
+        if it:
+            ctm.iterate()
+        for (x, y) in ctm.site_coords:
+            data[f"it{it}_rdm1x2_{x}{y}"] = ctm.compute_rdm1x2(x, y).toarray()
+            data[f"it{it}_rdm2x1_{x}{y}"] = ctm.compute_rdm2x1(x, y).toarray()
+        data[f"it{it}_chi"] = np.array(ctm.chi_values)
+        data[f"it{it}_logZ"] = np.array(ctm.compute_PEPS_norm_log())
+    save("ctmrg_u1_random", data)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1:
+        for name in sys.argv[1:]:
+            globals()["case_" + name]()
+        sys.exit(0)
     case_u1_reference_test()
     case_z2_rank6()
     case_u1_microbench_small()
     case_find_block_cuts()
     case_ising()
+    case_ctmrg_u1()
