@@ -311,6 +311,45 @@ def case_ctmrg_u1():
     save("ctmrg_u1_random", data)
 
 
+SDS_22 = np.array(
+    [[0.25, 0.0, 0.0, 0.0], [0.0, -0.25, 0.5, 0.0], [0.0, 0.5, -0.25, 0.0],
+     [0.0, 0.0, 0.0, 0.25]]
+)
+
+
+def case_simple_update_u1():
+    """Heisenberg spin-1/2 on the square lattice, U(1) symmetric simple update
+    (examples/heisenberg_simple_update.py:67-82 with D=6), then CTMRG on the
+    resulting tensors."""
+    from frostspin.ctmrg import SequentialCTMRG
+    from frostspin.simple_update import SimpleUpdate
+
+    reps = (np.array([1, -1], dtype=np.int8),) * 2
+    h = U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 6, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    data = {"D": np.array(6), "tau": np.array(0.01)}
+    pack_tensor("h", h, data)
+    for k, beta in enumerate((0.2, 0.4)):
+        su.evolve(0.2)
+        data[f"b{k}_beta"] = np.array(su.beta)
+        data[f"b{k}_logZ"] = np.array(su.logZ)
+        for i, w in enumerate(su.get_weights()):
+            data[f"b{k}_w{i}"] = w
+        for i, r in enumerate(su.get_bond_representations()):
+            data[f"b{k}_rep{i}"] = r
+    tensors = su.get_tensors()
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 16, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for it in range(3):
+        ctm.iterate()
+    for (x, y) in ctm.site_coords:
+        data[f"rdm1x2_{x}{y}"] = ctm.compute_rdm1x2(x, y).toarray()
+        data[f"rdm2x1_{x}{y}"] = ctm.compute_rdm2x1(x, y).toarray()
+    data["logZ_ctm"] = np.array(ctm.compute_PEPS_norm_log())
+    save("simple_update_u1", data)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
@@ -322,3 +361,4 @@ if __name__ == "__main__":
     case_find_block_cuts()
     case_ising()
     case_ctmrg_u1()
+    case_simple_update_u1()
