@@ -145,6 +145,7 @@ SIGNATURES = {
     "fs_ozaki_gemm_noalloc": (ctypes.c_int, [_P, _I64, _I32, _P]),
     "fs_scale": (ctypes.c_int, [_P, _I64, _D, _P]),
     "fs_axpby": (ctypes.c_int, [_P, _P, _I64, _D, _D, _P]),
+    "fs_scale_by": (ctypes.c_int, [_P, _I64, _P, _I32, _P]),
     "fs_pow": (ctypes.c_int, [_P, _P, _I64, _D, _P]),
     "fs_reduce_partials": (ctypes.c_int, []),
     "fs_weighted_sumsq": (ctypes.c_int, [_P, _P, _I64, _P, _I64, _P, _P]),

@@ -15,6 +15,14 @@ __global__ void k_scale(double* __restrict__ x, int64_t n, double alpha) {
         x[i] *= alpha;
 }
 
+__global__ void k_scale_by(double* __restrict__ x, int64_t n, const double* __restrict__ s,
+                           int invert) {
+    const double a = invert ? 1.0 / s[0] : s[0];
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        x[i] *= a;
+}
+
 __global__ void k_axpby(const double* __restrict__ x, double* __restrict__ y, int64_t n,
                         double a, double b) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -161,6 +169,16 @@ extern "C" int fs_scale(double* d_x, int64_t n, double alpha, void* stream) {
     if (d_x == nullptr) return FS_ERR_INVALID_ARG;
     fsb::k_scale<<<fsb::elementwise_grid(n), fsb::kOpThreads, 0, fsb::as_stream(stream)>>>(
         d_x, n, alpha);
+    return fsb::launch_status();
+}
+
+extern "C" int fs_scale_by(double* d_x, int64_t n, const double* d_scalar, int32_t invert,
+                           void* stream) {
+    if (n < 0) return FS_ERR_INVALID_ARG;
+    if (n == 0) return FS_OK;
+    if (d_x == nullptr || d_scalar == nullptr) return FS_ERR_INVALID_ARG;
+    fsb::k_scale_by<<<fsb::elementwise_grid(n), fsb::kOpThreads, 0, fsb::as_stream(stream)>>>(
+        d_x, n, d_scalar, invert);
     return fsb::launch_status();
 }
 

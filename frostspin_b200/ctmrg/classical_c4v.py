@@ -22,14 +22,14 @@ def iterate_c4v(s, T, a, a2, chi_target):
     matC = a2 @ matC
     matC = matC.permute((0, 2), (1, 3))
     news, U = matC.truncated_eigh(chi_target)
-    news /= news.norm()
+    news /= news.norm_device()
     newT = U.permute((1,), (0, 2))
     newT = Tp @ newT
     newT = newT.permute((1, 2), (0, 3))
     newT = a @ newT
     newT = newT.permute((0, 2), (1, 3))
     newT = U.dagger() @ newT
-    newT /= newT.norm()
+    newT /= newT.norm_device()
     return news, newT
 
 

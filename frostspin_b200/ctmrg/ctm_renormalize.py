@@ -112,28 +112,28 @@ def renormalize_T(Pt, T, A, P):
     nT = A.permute((0, 1, 4, 5), (2, 3)).dagger() @ nT
     nT = nT.permute((3, 1, 4), (2, 0, 5))
     nT = Pt.transpose() @ nT
-    nT /= nT.norm()
+    nT /= nT.norm_device()
     return nT
 
 
 def renormalize_corner_P(C, T, P):
     """ctm_renormalize.py:169-193."""
     nC = (T @ C).permute((0,), (1, 2, 3)) @ P
-    nC /= nC.norm()
+    nC /= nC.norm_device()
     return nC
 
 
 def renormalize_corner_Pt(C, T, Pt):
     """ctm_renormalize.py:196-216."""
     nC = (T @ C).permute((0,), (1, 2, 3)) @ Pt
-    nC /= nC.norm()
+    nC /= nC.norm_device()
     return nC
 
 
 def renormalize_quadrant(P, quadrant, Pt):
     """ctm_renormalize.py:219-225."""
     nc = P.transpose() @ quadrant @ Pt
-    nc /= nc.norm()
+    nc /= nc.norm_device()
     return nc
 
 

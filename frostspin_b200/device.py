@@ -10,14 +10,17 @@ import torch
 from . import _native
 
 _scratch = {}
+_available = []
 
 
 def device():
     """The CUDA device tensors live on.  Raises when CUDA is unavailable: there is
     no CPU fallback for any symmetric-tensor operation."""
-    if not torch.cuda.is_available():
-        msg = "frostspin_b200 needs a CUDA device (B200, sm_100a); none is available"
-        raise RuntimeError(msg)
+    if not _available:
+        if not torch.cuda.is_available():
+            msg = "frostspin_b200 needs a CUDA device (B200, sm_100a); none is available"
+            raise RuntimeError(msg)
+        _available.append(True)
     return torch.device("cuda", torch.cuda.current_device())
 
 
@@ -32,17 +35,19 @@ def ptr(t):
 
 def upload(arr):
     """Copy a numpy array (any dtype, structured included) into a new uint8 device
-    buffer; the result owns its memory and must outlive the kernels reading it."""
+    buffer.  The bytes go through pinned host memory (torch's caching host
+    allocator keeps that block alive until the copy has run), so the copy is
+    asynchronous and the host does not wait for the stream."""
     a = np.ascontiguousarray(arr)
     raw = torch.from_numpy(a.view(np.uint8).reshape(-1))
     if raw.numel() == 0:
         return torch.empty(0, dtype=torch.uint8, device=device())
-    return raw.to(device(), non_blocking=False)
+    return raw.pin_memory().to(device(), non_blocking=True)
 
 
 def upload_f64(arr):
     a = np.ascontiguousarray(arr, dtype=np.float64)
-    return torch.from_numpy(a).to(device())
+    return torch.from_numpy(a).pin_memory().to(device(), non_blocking=True)
 
 
 def scratch_partials():

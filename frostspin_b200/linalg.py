@@ -357,7 +357,18 @@ def axpby(x, y, a, b):
 
 
 def scale_(x, alpha):
-    _native.call("fs_scale", dev.ptr(x), x.numel(), float(alpha), dev.stream())
+    """x *= alpha; alpha a number, or a 1-element device tensor (no host sync)."""
+    if isinstance(alpha, torch.Tensor):
+        s = alpha.reshape(1).to(torch.float64)
+        _native.call("fs_scale_by", dev.ptr(x), x.numel(), s.data_ptr(), 0, dev.stream())
+    else:
+        _native.call("fs_scale", dev.ptr(x), x.numel(), float(alpha), dev.stream())
+
+
+def divide_(x, s):
+    """x /= s for a 1-element device tensor s (no host sync)."""
+    s = s.reshape(1).to(torch.float64)
+    _native.call("fs_scale_by", dev.ptr(x), x.numel(), s.data_ptr(), 1, dev.stream())
 
 
 def power(x, p):

@@ -10,7 +10,7 @@ import numpy as np
 import torch
 
 
-def truncated_svd_block(m, k, *, full, n_iter=6, oversampling=None):
+def truncated_svd_block(m, k, *, full, n_iter=3, oversampling=None):
     """Leading singular triplets of one device block.
 
     full=True: dense SVD (cuSOLVER), all values, like the reference's robust_svd

@@ -174,6 +174,10 @@ class DiagonalTensor:
         raise NotImplementedError("Invalid type for /")
 
     def __itruediv__(self, x):
+        if isinstance(x, torch.Tensor):
+            if self._data.numel():
+                linalg.divide_(self._data, x)
+            return self
         self *= 1.0 / x
         return self
 

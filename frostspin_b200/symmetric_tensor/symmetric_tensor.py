@@ -407,10 +407,13 @@ class SymmetricTensor:
         return self
 
     def __itruediv__(self, x):
-        if isinstance(x, torch.Tensor):
-            x = float(x)
+        """In place division; x may be a number or a 1-element device tensor
+        (for example norm_device()), which avoids a host synchronisation."""
         if self._data.numel():
-            linalg.scale_(self._data, 1.0 / float(x))
+            if isinstance(x, torch.Tensor):
+                linalg.divide_(self._data, x)
+            else:
+                linalg.scale_(self._data, 1.0 / float(x))
         return self
 
     def __matmul__(self, other):

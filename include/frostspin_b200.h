@@ -229,6 +229,12 @@ int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_problems,
  * (symmetric_tensor.py:441-451) and scalar __mul__ (:377-424). */
 int fs_scale(double* d_x, int64_t n, double alpha, void* stream);
 
+/* x[0:n] *= s (invert == 0) or x[0:n] /= s (invert != 0) with s = d_scalar[0]
+ * read on the device: normalisation by a device-computed norm without a host
+ * round trip (the `t /= t.norm()` steps of ctm_renormalize.py:165, :192, :215). */
+int fs_scale_by(double* d_x, int64_t n, const double* d_scalar, int32_t invert,
+                void* stream);
+
 /* y[0:n] = a*x + b*y.  Replaces the block sums of __add__/__sub__
  * (symmetric_tensor.py:326-352). */
 int fs_axpby(const double* d_x, double* d_y, int64_t n, double a, double b,
