@@ -2,7 +2,17 @@
 """Benchmark driver: prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload u1_microbench]
+                    [--workload ctmrg|u1_microbench] [--precision fp64|ozakiS]
+
+Workload "ctmrg" (default): double-layer CTMRG of the spin-1/2 Heisenberg
+model on the square lattice.  The site tensors come from the finite-temperature
+simple update (2-site checkerboard cell, tau = 0.01, second-order Trotter,
+bond dimension target D, U(1) symmetry) evolved to beta = 2 on the device; then
+SequentialCTMRG on the AB/BA cell at corner dimension chi.  One step = one CTMRG
+iteration (up, right, down, left moves).  The timed iterations start from an
+environment warmed up for W iterations; the same K iterations run once with
+the plain FP64 grouped GEMM and once with the tcgen05 Ozaki GEMM from copies of
+that environment, and the energy per bond of both runs is compared.
 
 Workload "u1_microbench": the U(1) kernel microbenchmark -- rank-4 float64
 tensors whose legs carry charges -4..4 with degeneracies ~ exp(-q^2/8) rounded
@@ -255,6 +265,220 @@ def cpu_baseline_full_step(full_ncoeff, full_flops, sample_states=128):
         ),
     }
 
+
+
+# ------------------------------------------------------------ CTMRG workload
+
+SDS_22 = np.array([[0.25, 0.0, 0.0, 0.0], [0.0, -0.25, 0.5, 0.0], [0.0, 0.5, -0.25, 0.0],
+                   [0.0, 0.0, 0.0, 0.25]])
+
+
+def heisenberg_u1():
+    from frostspin_b200 import U1SymmetricTensor
+
+    reps = (np.array([1, -1], dtype=np.int8),) * 2
+    return U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
+
+
+def energy_per_bond(ctm):
+    """Mean of tr(rho h) over the 4 inequivalent bonds of the AB/BA cell."""
+    h = SDS_22.reshape(2, 2, 2, 2)
+    es = []
+    for x, y in ctm.site_coords:
+        for r in (ctm.compute_rdm1x2(x, y), ctm.compute_rdm2x1(x, y)):
+            es.append(float(np.einsum("ijkl,klij->", r.toarray(), h)))
+    return float(np.mean(es))
+
+
+def ctmrg_setup(args):
+    import torch
+
+    from frostspin_b200.ctmrg import SequentialCTMRG
+    from frostspin_b200.simple_update import SimpleUpdate
+
+    t0 = time.perf_counter()
+    su = SimpleUpdate.square_lattice_first_neighbor(heisenberg_u1(), args.D, 0.01,
+                                                    rcutoff=1e-10, degen_ratio=0.9999)
+    su.evolve(args.beta)
+    tensors = su.get_tensors()
+    torch.cuda.synchronize()
+    t_su = time.perf_counter() - t0
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, args.chi, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    return su, tensors, ctm, t_su
+
+
+def timed_iterations(ctm, steps, precision, local):
+    import torch
+
+    from frostspin_b200 import _native, instrument, linalg
+
+    linalg.set_gemm_precision(precision)
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    n0 = _native.kernel_launches()
+    instrument.enable()
+    clocks.start()
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        ctm.iterate()
+    e.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    instrument.disable()
+    kernels = instrument.summary()
+    launches = _native.kernel_launches() - n0
+    linalg.check_ozaki_flags()
+    return s.elapsed_time(e) * 1e-3, clk, kernels, launches
+
+
+def run_ctmrg(args, world, rank, local):
+    import torch
+
+    from frostspin_b200 import U1SymmetricTensor, linalg
+
+    mixed = args.precision if args.precision != "fp64" else "ozaki6"
+    su, tensors, ctm, t_su = ctmrg_setup(args)
+    linalg.set_gemm_precision("fp64")
+    for _ in range(args.warmup):
+        ctm.iterate()
+    torch.cuda.synchronize()
+    start_env = ctm.copy()
+    barrier(world)
+    t64, clk64, k64, l64 = timed_iterations(ctm, args.steps, "fp64", local)
+    e64 = energy_per_bond(ctm)
+    ctm_mixed = start_env.copy()
+    barrier(world)
+    tmx, clkmx, kmx, lmx = timed_iterations(ctm_mixed, args.steps, mixed, local)
+    emx = energy_per_bond(ctm_mixed)
+    t64 = max_over_ranks(t64, world)
+    tmx = max_over_ranks(tmx, world)
+    headline_mixed = args.precision != "fp64"
+    t_head = tmx if headline_mixed else t64
+    kern = kmx if headline_mixed else k64
+
+    # end to end through the public API: site tensors uploaded from pinned host
+    # buffers each step, energy (reduced density matrices) read back
+    hostA = [t.data.cpu().pin_memory() for t in tensors]
+    e2e_env = start_env.copy()
+    linalg.set_gemm_precision(mixed if headline_mixed else "fp64")
+    e2e_steps = max(1, min(args.steps, 2))
+    torch.cuda.synchronize()
+    es = torch.cuda.Event(enable_timing=True)
+    ee = torch.cuda.Event(enable_timing=True)
+    es.record()
+    for _ in range(e2e_steps):
+        new = [U1SymmetricTensor.from_flat(t.row_reps, t.col_reps, h, t.block_irreps, t.signature)
+               for t, h in zip(tensors, hostA, strict=True)]
+        e2e_env.set_tensors(new)
+        e2e_env.iterate()
+        energy_per_bond(e2e_env)
+    ee.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
+    h2d = int(sum(h.numel() * 8 for h in hostA))
+    d2h = int(4 * 2 * 16 * 8)  # four 2x2x2x2 reduced density matrices per site pair
+
+    hbm, bf16, peak_kind = load_peaks()
+    fp64_peak = measure_dgemm_peak()
+    gem = kern.get("gemm_ozaki") if headline_mixed else kern.get("gemm_fp64")
+    if gem is None:
+        gem = kern.get("gemm_fp64", {"ms": 1.0, "flops": 0.0, "launches": 0})
+    perm = kern.get("permute", {"ms": 1.0, "bytes": 0.0, "launches": 0})
+    if headline_mixed and "gemm_ozaki" in kern:
+        ach = gem["int8_ops"] / (gem["ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "k_oz_gemm (+ k_oz_split, k_oz_exponents)",
+                "achieved": ach, "peak": 2.0 * bf16, "unit": "TOP/s (int8)",
+                "frac": ach / (2.0 * bf16),
+                "peak_kind": f"2 x {peak_kind} bf16 dense (int8 dense rate is twice bf16)",
+                "traffic": None, "launches": gem["launches"], "ms": gem["ms"],
+                "effective_fp64_tflops": gem["flops"] / (gem["ms"] * 1e-3) / 1e12}
+    else:
+        ach = gem["flops"] / (gem["ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "k_grouped_dgemm", "achieved": ach,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
+                "peak_kind": "measured in-run cuBLAS DGEMM 8192^3", "traffic": None,
+                "launches": gem["launches"], "ms": gem["ms"]}
+    perm_gbs = perm["bytes"] / (perm["ms"] * 1e-3) / 1e9
+    value = world * args.steps / t_head
+    line = {
+        "metric": "CTMRG iter/s, grouped mixed-precision vs plain FP64 on 1 B200",
+        "value": value,
+        "unit": "iter/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_head / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if not headline_mixed else f"f64 via int8 {mixed}",
+        "data": "synthetic (site tensors from the device simple update, seeded)",
+        "impl": "ours",
+        "config": {
+            "workload": "ctmrg_heisenberg_u1",
+            "model": "spin-1/2 Heisenberg square lattice, AB/BA cell, U(1) sectors",
+            "beta": args.beta, "D_target": args.D, "Dmax": su.Dmax, "chi": args.chi,
+            "chi_values": [int(c) for c in ctm.chi_values],
+            "precision": mixed if headline_mixed else "fp64",
+            "fp64_iter_per_s": world * args.steps / t64,
+            "mixed_iter_per_s": world * args.steps / tmx,
+            "mixed_over_fp64": t64 / tmx,
+            "energy_fp64": e64, "energy_mixed": emx,
+            "energy_rel_err_mixed_vs_fp64": abs(emx - e64) / abs(e64),
+            "kernels_fp64_run": {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in k64.items()},
+            "kernels_mixed_run": {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in kmx.items()},
+            "simple_update_setup_s": t_su,
+            "l2": "working set > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": roof,
+        "roofline_permute": {"bound": "hbm", "kernel": "k_perm_gather", "achieved": perm_gbs,
+                             "peak": hbm, "unit": "GB/s", "frac": perm_gbs / hbm,
+                             "launches": perm["launches"], "ms": perm["ms"]},
+        "e2e": {"value": world * e2e_steps / t_e2e, "unit": "iter/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": lmx if headline_mixed else l64,
+        "clocks": clkmx if headline_mixed else clk64,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        t_cpu, info = cpu_ctmrg_seconds(tensors, ctm_mixed, args.chi)
+        info["value"] = 1.0 / t_cpu
+        info["unit"] = "iter/s"
+        line["cpu_baseline"] = info
+    return line
+
+
+def env_to_oracle(dev_ctm, chi):
+    """Oracle CTMRG warm-started from a device environment (host copies)."""
+    from oracle import ctmrg_oracle as co
+    from oracle import frostspin_oracle as fo
+
+    def ot(t):
+        return co.OT(fo.OTensor(t.row_reps, t.col_reps, t.host_blocks(), t.block_irreps,
+                                t.signature))
+
+    env = dev_ctm.environment
+    A, B = env.elementary_tensors
+    oc = co.SequentialCTMRG(ot(A).o, ot(B).o, chi, cutoff=1e-10, degen_ratio=0.9999)
+    for name in ("C1", "C2", "C3", "C4", "T1", "T2", "T3", "T4"):
+        oc.t[name] = [ot(t) for t in env.tensors(name)]
+    return oc
+
+
+def cpu_ctmrg_seconds(tensors, dev_ctm, chi):
+    """One iteration of the numpy oracle CTMRG (restating the reference), warm
+    started from the device environment at the same chi and D."""
+    oc = env_to_oracle(dev_ctm, chi)
+    t0 = time.perf_counter()
+    oc.iterate()
+    t = time.perf_counter() - t0
+    return t, {"cores": os.cpu_count() or 1, "kind": "port",
+               "sample": (f"one iteration of the numpy oracle SequentialCTMRG (dense "
+                          f"sector SVDs, BLAS with all host threads) at the same D and "
+                          f"chi={chi}, warm-started from the device environment: {t:.2f} s")}
 
 # ------------------------------------------------------------------- driver
 
@@ -512,9 +736,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["u1_microbench"], default="u1_microbench")
+    ap.add_argument("--workload", choices=["ctmrg", "u1_microbench"], default="ctmrg")
+    ap.add_argument("--D", type=int, default=12, help="simple-update bond dimension target")
+    ap.add_argument("--chi", type=int, default=64, help="CTMRG corner dimension target")
+    ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64",
+    ap.add_argument("--precision", default="ozaki6",
                     help="sector GEMM arithmetic: fp64 or ozakiS (S = 3..8 int8 slices)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
                     help="states per leg (256 = the benchmark; smaller for profiling)")
@@ -529,7 +756,10 @@ def main():
             print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_init(args.gpus)
-    line = run_ours(args, world, rank, local)
+    if args.workload == "ctmrg":
+        line = run_ctmrg(args, world, rank, local)
+    else:
+        line = run_ours(args, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -188,10 +188,27 @@ def check(status, what):
         raise NativeError(msg)
 
 
+# number of calls per entry point (bench.py reports the kernel launches of its
+# timed region from these counters)
+CALL_COUNTS = {}
+
+# kernels each entry point launches
+LAUNCHES_PER_CALL = {
+    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1,
+    "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
+    "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1,
+}
+
+
+def kernel_launches():
+    return sum(LAUNCHES_PER_CALL.get(k, 0) * v for k, v in CALL_COUNTS.items())
+
+
 def call(name, *args):
     """Call a C ABI function by name and raise on a non-zero status."""
     st = getattr(lib(), name)(*args)
     check(st, name)
+    CALL_COUNTS[name] = CALL_COUNTS.get(name, 0) + 1
     return st
 
 

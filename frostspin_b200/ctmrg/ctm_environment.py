@@ -99,6 +99,25 @@ class CTMEnvironment:
                 envs[k].append(d[k])
         return cls(cell, tensors, envs)
 
+    def copy(self):
+        """Independent environment: every tensor's blocks are copied."""
+        envs = {k: [t.copy() for t in self._t[k]] for k in _NAMES}
+        return type(self)(self._cell, self._As, envs)
+
+    def set_tensors(self, tensors):
+        """New elementary tensors with the same representations; the environment
+        is kept and the enlarged corners are reset (ctm_environment.py:299-312)."""
+        if len(tensors) != self._n_sites:
+            raise ValueError("Incompatible cell and tensors")
+        for i, A in enumerate(tensors):
+            if not A.match_representations(self._As[i]):
+                raise ValueError("Incompatible representation for new tensor")
+        self._As = tuple(tensors)
+        self.reset_constructed_corners()
+
+    def tensors(self, name):
+        return list(self._t[name])
+
     # ------------------------------------------------------------ accessors
     def _index(self, x, y):
         return self._indices[x % self._Lx, y % self._Ly]

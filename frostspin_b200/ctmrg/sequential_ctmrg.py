@@ -83,6 +83,20 @@ class SequentialCTMRG:
         data |= self._env.get_data_dic()
         np.savez_compressed(filename, **data, **additional_data)
 
+    def copy(self):
+        """Independent copy (environment tensors copied, parameters shared)."""
+        return type(self)(self._env.copy(), self.chi_target, verbosity=self.verbosity,
+                          block_chi_ratio=self.block_chi_ratio, ncv_ratio=self.ncv_ratio,
+                          cutoff=self.cutoff, degen_ratio=self.degen_ratio)
+
+    def set_tensors(self, tensors):
+        """abstract_ctmrg.py:158-166."""
+        self._env.set_tensors(tensors)
+
+    @property
+    def environment(self):
+        return self._env
+
     # -------------------------------------------------------------- properties
     @property
     def Lx(self):

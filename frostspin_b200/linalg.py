@@ -12,6 +12,7 @@ import torch
 
 from . import _native
 from . import device as dev
+from . import instrument
 
 # ----------------------------------------------------------------- precision
 
@@ -85,12 +86,53 @@ def grouped_gemm(problems):
         arr["beta"][i] = p.get("beta", 0.0)
         ntile.append(((M + tm - 1) // tm) * ((N + tn - 1) // tn))
     mode = gemm_precision()
+    ntile = np.array(ntile, dtype=np.int64)
+    flops = 2.0 * (arr["M"].astype(np.float64) * arr["N"] * arr["K"])
     if mode == "fp64":
-        _dgemm(arr, problems, tm, tn, np.array(ntile, dtype=np.int64))
+        with instrument.region("gemm_fp64", flops=float(flops.sum())):
+            _dgemm(arr, problems, tm, tn, ntile)
     elif mode.startswith("ozaki"):
-        ozaki_gemm(arr, int(mode[5:]))
+        S = int(mode[5:])
+        use = ozaki_pays(arr, S)
+        if use.any():
+            with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
+                                   int8_ops=ozaki_int8_ops(arr[use], S)):
+                ozaki_gemm(arr[use], S)
+        if (~use).any():
+            with instrument.region("gemm_fp64", flops=float(flops[~use].sum())):
+                _dgemm(arr[~use], None, tm, tn, ntile[~use])
     else:  # pragma: no cover - guarded by set_gemm_precision
         raise ValueError(mode)
+
+
+# rough rates of the two paths on B200 (measured on the U(1) microbench), used
+# only to decide which path a sector GEMM takes in a mixed-precision run
+_INT8_OPS = 1.1e15
+_FP64_FLOPS = 1.1e13
+_EPILOGUE_BPS = 2.0e12
+_SPLIT_BPS = 3.0e12
+
+
+def _pad(x, a):
+    return (x + a - 1) // a * a
+
+
+def ozaki_int8_ops(arr, S):
+    M = _pad(arr["M"].astype(np.float64), 128)
+    N = _pad(arr["N"].astype(np.float64), 256)
+    K = _pad(np.maximum(arr["K"].astype(np.float64), 1), 128)
+    return float((2 * M * N * K).sum() * S * (S + 1) / 2)
+
+
+def ozaki_pays(arr, S):
+    """Per problem: True when the tcgen05 path is estimated faster than FP64."""
+    M = arr["M"].astype(np.float64)
+    N = arr["N"].astype(np.float64)
+    K = arr["K"].astype(np.float64)
+    t_oz = (S * (S + 1) / 2 * 2 * _pad(M, 128) * _pad(N, 256) * _pad(np.maximum(K, 1), 128)
+            / _INT8_OPS + S * M * N * 16 / _EPILOGUE_BPS + (M * K + K * N) * (8 + S) / _SPLIT_BPS)
+    t_64 = 2 * M * N * K / _FP64_FLOPS
+    return t_oz < t_64
 
 
 def _tile_table(arr, tm, tn, ntile):

@@ -13,6 +13,7 @@ import torch
 
 from .. import _native
 from .. import device as dev
+from .. import instrument
 from .abelian_plan import (
     GroupInfo,
     build_abelian_permute_plan,
@@ -187,17 +188,18 @@ class AbelianSymmetricTensor(SymmetricTensor):
             if plan.device_tables is None:
                 plan.device_tables = (dev.upload(plan.ebs), dev.upload(plan.tasks))
             d_ebs, d_tasks = plan.device_tables
-            _native.call(
-                "fs_abelian_permute",
-                dev.ptr(self._data),
-                int(self._data.numel()),
-                dev.ptr(out),
-                int(out.numel()),
-                d_ebs.data_ptr(),
-                int(plan.ebs.size),
-                d_tasks.data_ptr(),
-                int(plan.tasks.size),
-                None,
-                dev.stream(),
-            )
+            with instrument.region("permute", bytes=16.0 * plan.size):
+                _native.call(
+                    "fs_abelian_permute",
+                    dev.ptr(self._data),
+                    int(self._data.numel()),
+                    dev.ptr(out),
+                    int(out.numel()),
+                    d_ebs.data_ptr(),
+                    int(plan.ebs.size),
+                    d_tasks.data_ptr(),
+                    int(plan.tasks.size),
+                    None,
+                    dev.stream(),
+                )
         return out, plan.offsets, plan.block_shapes, plan.block_irreps

@@ -350,6 +350,24 @@ def case_simple_update_u1():
     save("simple_update_u1", data)
 
 
+def case_heisenberg_d12_beta2():
+    """Site tensors of the CTMRG benchmark: the reference's U(1) simple update of
+    the Heisenberg model, D=12, tau=0.01, evolved to beta=2 (get_tensors)."""
+    from frostspin.simple_update import SimpleUpdate
+
+    reps = (np.array([1, -1], dtype=np.int8),) * 2
+    h = U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 12, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    su.evolve(2.0)
+    data = {"beta": np.array(su.beta), "logZ": np.array(su.logZ)}
+    for i, w in enumerate(su.get_weights()):
+        data[f"w{i}"] = w
+    for i, t in enumerate(su.get_tensors()):
+        pack_tensor(f"A{i}", t, data)
+    save("heisenberg_d12_beta2", data)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:

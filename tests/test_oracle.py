@@ -129,3 +129,23 @@ def test_oracle_ising_energy_chi32():
         s_blocks, s_irr, T = fo.ising_c4v_iteration(s_blocks, s_irr, T, a, a2, 32)
     e = fo.ising_energy_per_bond(s_blocks, s_irr, T, a0d, mopd)
     assert abs(e - float(d["energy5"])) < 1e-9
+
+
+def test_oracle_ctmrg_matches_reference_run():
+    from oracle import ctmrg_oracle as co
+
+    d = load("ctmrg_u1_random")
+    A = oracle_from_dic(d, "A")
+    B = oracle_from_dic(d, "B")
+    ctm = co.SequentialCTMRG(A, B, 20)
+    for it in range(3):
+        if it:
+            ctm.iterate()
+        tol = 1e-12 if it == 0 else 1e-9
+        for x, y in ctm.coords:
+            r12 = co.ctm_rdm1x2(ctm, x, y)
+            r21 = co.ctm_rdm2x1(ctm, x, y)
+            ref12 = d[f"it{it}_rdm1x2_{x}{y}"]
+            ref21 = d[f"it{it}_rdm2x1_{x}{y}"]
+            assert np.abs(r12 - ref12).max() < tol * max(1.0, np.abs(ref12).max())
+            assert np.abs(r21 - ref21).max() < tol * max(1.0, np.abs(ref21).max())
