@@ -105,6 +105,20 @@ def grouped_gemm(problems):
         raise ValueError(mode)
 
 
+def grouped_dgemm_table(arr, region="gemm_fp64"):
+    """FP64 grouped GEMM over a prepared FsGemmProblem table (pointers already
+    set); always FP64, whatever the precision mode."""
+    if arr.size == 0:
+        return
+    tm, tn = _tile_shape()
+    M = arr["M"].astype(np.int64)
+    N = arr["N"].astype(np.int64)
+    ntile = ((M + tm - 1) // tm) * ((N + tn - 1) // tn)
+    flops = 2.0 * float((M.astype(np.float64) * N * arr["K"]).sum())
+    with instrument.region(region, flops=flops):
+        _dgemm(arr, None, tm, tn, ntile)
+
+
 # rough rates of the two paths on B200 (measured on the U(1) microbench), used
 # only to decide which path a sector GEMM takes in a mixed-precision run
 _INT8_OPS = 1.1e15

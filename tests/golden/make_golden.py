@@ -368,6 +368,96 @@ def case_heisenberg_d12_beta2():
     save("heisenberg_d12_beta2", data)
 
 
+def su2_rep(degen, irreps):
+    return np.array([degen, irreps], dtype=int)
+
+
+def _su2_permute_cases(t, perms, data, prefix):
+    for i, (ra, ca) in enumerate(perms):
+        p = t.permute(ra, ca)
+        pack_tensor(f"{prefix}perm{i}", p, data)
+        data[f"{prefix}perm{i}_axes"] = np.array(ra + ca)
+        data[f"{prefix}perm{i}_nrr"] = np.array(len(ra))
+        data[f"{prefix}perm{i}_dense"] = p.toarray()
+
+
+def case_su2():
+    """SU(2) fixtures.  Part 1 repeats the known-answer inputs of the
+    reference's tests/test_su2_tensor.py (S.S of two spins 1/2, the
+    external-degeneracy tensor, the missing-block tensor); part 2 is random
+    tensors with several irreps and degeneracies per leg, permuted in many ways,
+    plus transpose, dagger, matmul, norm and truncated SVD spectra."""
+    from frostspin import SU2SymmetricTensor
+
+    data = {}
+    r = su2_rep([1], [2])
+    sds = SDS_22.reshape(2, 2, 2, 2)
+    st = SU2SymmetricTensor.from_array(sds, (r, r), (r, r))
+    pack_tensor("sds", st, data)
+    data["sds_dense"] = sds
+    _su2_permute_cases(st, [((0, 1, 2), (3,)), ((3, 0, 2), (1,)), ((1, 3), (2, 0))],
+                       data, "sds_")
+    arrb = np.array([[-0.25, 0.0, 0.0, -0.5], [0.0, 0.25, 0.0, 0.0],
+                     [0.0, 0.0, 0.25, 0.0], [-0.5, 0.0, 0.0, -0.25]]).reshape(2, 2, 2, 2)
+    stb = SU2SymmetricTensor.from_array(arrb, (r, r), (r, r), signature=[0, 1, 1, 0])
+    pack_tensor("sdsb", stb, data)
+    data["sdsb_dense"] = arrb
+    _su2_permute_cases(stb, [((0, 1, 2), (3,)), ((3, 0, 2), (1,))], data, "sdsb_")
+
+    r1 = su2_rep([1], [1])
+    r12 = su2_rep([1, 2, 1], [1, 3, 5])
+    arr = np.eye(12).reshape(1, 12, 12, 1)
+    st3 = SU2SymmetricTensor.from_array(arr, (r1,), (r12, r12, r1), signature=[0, 0, 1, 1])
+    pack_tensor("ext", st3, data)
+    data["ext_dense"] = arr
+    _su2_permute_cases(st3, [((0, 1), (2, 3)), ((2, 0), (3, 1))], data, "ext_")
+
+    rng = np.random.default_rng(7)
+    r3 = su2_rep([1], [3])
+    t = SU2SymmetricTensor.random((r3, r3, r3), (r3,), rng=rng)
+    t = t @ t.dagger()
+    pack_tensor("miss", t, data)
+    _su2_permute_cases(t, [((3, 2, 1), (0, 5, 4)), ((0,), (1, 2, 3, 4, 5))], data, "miss_")
+
+    rng = np.random.default_rng(11)
+    ra = su2_rep([2, 1], [1, 3])
+    rb = su2_rep([1, 2], [2, 4])
+    rc = su2_rep([1, 1, 1], [1, 2, 3])
+    rd = su2_rep([2], [2])
+    re = su2_rep([1, 1], [1, 3])
+    sig = np.array([0, 1, 0, 1, 1], dtype=bool)
+    t = SU2SymmetricTensor.random((ra, rb), (rc, rd, re), signature=sig, rng=rng)
+    pack_tensor("r5", t, data)
+    data["r5_dense"] = t.toarray()
+    perms = [
+        ((3, 0, 2), (1, 4)),
+        ((3,), (1, 0, 4, 2)),
+        ((2, 3, 4), (0, 1)),
+        ((4, 1), (0, 3, 2)),
+        ((0, 1, 2, 3), (4,)),
+        ((1, 4, 0), (3, 2)),
+    ]
+    _su2_permute_cases(t, perms, data, "r5_")
+    pack_tensor("r5_transpose", t.transpose(), data)
+    pack_tensor("r5_dagger", t.dagger(), data)
+    data["r5_norm"] = np.array(t.norm())
+    m = t @ t.dagger()
+    pack_tensor("r5_matmul", m, data)
+    data["r5_matmul_trace"] = np.array(m.trace())
+    _, s, _ = m.truncated_svd(7)
+    pack_diag("r5_tsvd_s", s, data)
+
+    rng = np.random.default_rng(13)
+    rp = su2_rep([1], [2])
+    rv = su2_rep([1, 2, 1], [1, 2, 3])
+    sig6 = np.array([0, 0, 1, 1, 0, 1], dtype=bool)
+    t6 = SU2SymmetricTensor.random((rp, rp, rv), (rv, rv, rv), signature=sig6, rng=rng)
+    pack_tensor("r6", t6, data)
+    _su2_permute_cases(t6, [((0, 2, 4), (1, 3, 5)), ((5, 1), (0, 4, 3, 2)),
+                            ((2, 3, 0, 5, 1), (4,))], data, "r6_")
+    save("su2", data)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:

@@ -1,0 +1,158 @@
+"""Host logic of the SU(2) data plane, on the CPU.
+
+The permute and the dense conversions of an SU(2) tensor are one gather ->
+grouped GEMM -> scatter map (tables built on the host, applied on the device).
+Here the tables are applied by a numpy emulation of the kernels' index
+arithmetic and compared with outputs of the reference implementation
+(tests/golden/su2.npz): block structure bit-exact, values to 1e-13.
+The Clebsch-Gordan coefficients themselves are pinned against an independent
+closed-form evaluation.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from frostspin_b200.symmetric_tensor import su2_cg
+from frostspin_b200.symmetric_tensor.abelian_plan import emulate_permute
+from frostspin_b200.symmetric_tensor.su2_symmetric_tensor import (
+    SU2SymmetricTensor,
+    compute_fusion_tensor,
+)
+from tests.helpers import load
+
+TOL = 1e-13
+
+
+class _Tables:
+    def __init__(self, ebs, size):
+        self.ebs = ebs
+        self.size = size
+
+
+def emulate_map(m, src):
+    x = emulate_permute(_Tables(m.gather[0], m.x_size), src)
+    assert not np.isnan(x).any()
+    y_off = np.zeros(m.M.size, dtype=np.int64)
+    y_off[1:] = np.cumsum((m.M * m.N)[:-1])
+    y = np.empty(int((m.M * m.N).sum()))
+    for g in range(m.M.size):
+        M, N, K = int(m.M[g]), int(m.N[g]), int(m.K[g])
+        U = m.u_host[m.u_off[g] : m.u_off[g] + M * K].reshape(M, K)
+        X = x[m.x_off[g] : m.x_off[g] + K * N].reshape(K, N)
+        y[y_off[g] : y_off[g] + M * N] = (U @ X).ravel()
+    out = emulate_permute(_Tables(m.scatter[0], m.out_size), y)
+    if m.zero_out:
+        out = np.nan_to_num(out, nan=0.0)
+    assert not np.isnan(out).any()
+    return out
+
+
+def host_tensor(d, prefix, trans=False):
+    """Reference fixture -> SU2 tensor object whose buffer is a CPU torch tensor
+    (enough for building plans; never handed to a kernel)."""
+    nrr = int(d[prefix + "_n_row_reps"])
+    ncr = int(d[prefix + "_n_col_reps"])
+    rr = [d[f"{prefix}_row_rep_{i}"] for i in range(nrr)]
+    cr = [d[f"{prefix}_col_rep_{i}"] for i in range(ncr)]
+    irr = d[prefix + "_block_irreps"]
+    blocks = [d[f"{prefix}_block_{i}"] for i in range(irr.size)]
+    flat = [(b.T if trans else b).ravel() for b in blocks]
+    shapes = np.array([b.shape for b in blocks], dtype=np.int64).reshape(-1, 2)
+    offsets = np.zeros(len(blocks), dtype=np.int64)
+    if len(blocks) > 1:
+        offsets[1:] = np.cumsum(shapes[:-1, 0] * shapes[:-1, 1])
+    data = torch.from_numpy(np.concatenate(flat) if flat else np.zeros(0))
+    return SU2SymmetricTensor._from_storage(rr, cr, data, offsets, shapes, irr,
+                                            d[prefix + "_signature"], trans)
+
+
+def ref_blocks(d, prefix):
+    irr = d[prefix + "_block_irreps"]
+    return irr, [d[f"{prefix}_block_{i}"] for i in range(irr.size)]
+
+
+def permute_cases(d):
+    names = sorted({k.split("perm")[0] for k in d.files if "perm" in k and k.endswith("_axes")})
+    for base in names:
+        i = 0
+        while f"{base}perm{i}_axes" in d:
+            yield base.rstrip("_"), i
+            i += 1
+
+
+@pytest.mark.parametrize("trans", [False, True])
+def test_su2_permute_tables_match_reference(trans):
+    d = load("su2")
+    n = 0
+    for base, i in permute_cases(d):
+        t = host_tensor(d, base, trans=trans)
+        pre = f"{base}_perm{i}"
+        axes = tuple(int(a) for a in d[pre + "_axes"])
+        nrr = int(d[pre + "_nrr"])
+        m = t._permute_map(axes, nrr)
+        out = emulate_map(m, t.data.numpy())
+        irr, blocks = ref_blocks(d, pre)
+        assert np.array_equal(m.out_irreps, irr), pre
+        assert len(blocks) == m.out_shapes.shape[0]
+        scale = max(np.abs(b).max() for b in blocks)
+        for o, (r, c), b in zip(m.out_offsets, m.out_shapes, blocks, strict=True):
+            assert (r, c) == b.shape, pre
+            got = out[o : o + r * c].reshape(r, c)
+            assert np.abs(got - b).max() <= TOL * scale, pre
+        n += 1
+    assert n >= 15
+
+
+def test_su2_dense_conversions_match_reference():
+    d = load("su2")
+    for base in ("sds", "sdsb", "ext", "r5"):
+        t = host_tensor(d, base)
+        dense = d[base + "_dense"]
+        # blocks -> dense
+        got = emulate_map(t._to_dense_map(), t.data.numpy())
+        assert np.abs(got - dense.ravel()).max() <= TOL * max(np.abs(dense).max(), 1)
+        # dense -> blocks
+        m = SU2SymmetricTensor._from_dense_map(t.row_reps, t.col_reps, t.signature)
+        out = emulate_map(m, dense.ravel())
+        irr, blocks = ref_blocks(d, base)
+        assert np.array_equal(m.out_irreps, irr)
+        for o, (r, c), b in zip(m.out_offsets, m.out_shapes, blocks, strict=True):
+            assert np.abs(out[o : o + r * c].reshape(r, c) - b).max() <= TOL * max(
+                np.abs(b).max(), 1
+            )
+
+
+def test_su2_known_answer_blocks():
+    """tests/test_su2_tensor.py:117-123 of the reference: S.S of two spins 1/2 has
+    blocks -3/4 (singlet) and 1/4 (triplet)."""
+    d = load("su2")
+    irr, blocks = ref_blocks(d, "sds")
+    assert np.array_equal(irr, [1, 3])
+    assert abs(blocks[0][0, 0] + 0.75) < 1e-14
+    assert abs(blocks[1][0, 0] - 0.25) < 1e-14
+
+
+def test_su2_structure_functions():
+    r = np.array([[1, 2], [1, 3]])
+    assert np.array_equal(SU2SymmetricTensor.combine_representations((r, r), None),
+                          [[5, 8, 4], [1, 3, 5]])
+    irr, shapes = SU2SymmetricTensor.get_block_sizes(
+        (r, r), (r,), np.array([False, False, True])
+    )
+    assert np.array_equal(irr, [1, 3])
+    assert np.array_equal(shapes, [[5, 1], [8, 2]])
+    rep, proj = compute_fusion_tensor(np.array([[1], [2]]), np.array([[1], [2]]), False, False)
+    assert np.array_equal(rep, [[1, 1], [1, 3]])
+    # the fusion tensor is an isometry: P^T P = 1
+    p = proj.reshape(4, 4)
+    assert np.abs(p.T @ p - np.eye(4)).max() < 1e-15
+
+
+def test_cg_coefficients_against_closed_form():
+    for d1 in range(1, 6):
+        for d2 in range(1, 6):
+            for d3 in range(abs(d1 - d2) + 1, d1 + d2, 2):
+                a = su2_cg.cg_tensor(d1, d2, d3)
+                b = su2_cg.cg_tensor_racah(d1, d2, d3)
+                assert np.abs(a - b).max() <= 2.3e-16
