@@ -350,6 +350,42 @@ def case_simple_update_u1():
     save("simple_update_u1", data)
 
 
+def case_simple_update_su2():
+    """The same Heisenberg simple update with SU(2) symmetry (D=8 states),
+    then SU(2) SequentialCTMRG on the resulting tensors."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.ctmrg import SequentialCTMRG
+    from frostspin.simple_update import SimpleUpdate
+
+    r = np.array([[1], [2]])
+    h = SU2SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), (r, r), (r, r))
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 8, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    data = {"D": np.array(8), "tau": np.array(0.01)}
+    pack_tensor("h", h, data)
+    for k in range(2):
+        su.evolve(0.2)
+        data[f"b{k}_beta"] = np.array(su.beta)
+        data[f"b{k}_logZ"] = np.array(su.logZ)
+        for i, w in enumerate(su.get_weights()):
+            data[f"b{k}_w{i}"] = w
+        for i, rep in enumerate(su.get_bond_representations()):
+            data[f"b{k}_rep{i}"] = rep
+    tensors = su.get_tensors()
+    for i, t in enumerate(tensors):
+        pack_tensor(f"A{i}", t, data)
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for it in range(3):
+        ctm.iterate()
+        data[f"it{it}_chi"] = np.array(ctm.chi_values)
+    for (x, y) in ctm.site_coords:
+        data[f"rdm1x2_{x}{y}"] = ctm.compute_rdm1x2(x, y).toarray()
+        data[f"rdm2x1_{x}{y}"] = ctm.compute_rdm2x1(x, y).toarray()
+    data["logZ_ctm"] = np.array(ctm.compute_PEPS_norm_log())
+    save("simple_update_su2", data)
+
+
 def case_heisenberg_d12_beta2():
     """Site tensors of the CTMRG benchmark: the reference's U(1) simple update of
     the Heisenberg model, D=12, tau=0.01, evolved to beta=2 (get_tensors)."""

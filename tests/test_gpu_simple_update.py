@@ -38,3 +38,35 @@ def test_simple_update_then_ctmrg_matches_reference():
             got = fn(x, y).toarray()
             assert np.abs(got - d[f"{kind}_{x}{y}"]).max() < 1e-8
     assert abs(ctm.compute_PEPS_norm_log() - float(d["logZ_ctm"])) < 1e-8
+
+
+def test_su2_simple_update_then_ctmrg_matches_reference():
+    """The same chain with SU(2) symmetry (D=8 states, chi=20): weights, logZ and
+    bond representations after beta = 0.2 and 0.4, the CTMRG chi after each
+    iteration (bit-identical truncation decisions), then the rdms."""
+    from frostspin_b200 import SU2SymmetricTensor
+    from frostspin_b200.ctmrg import SequentialCTMRG
+    from frostspin_b200.simple_update import SimpleUpdate
+
+    d = load("simple_update_su2")
+    h = SU2SymmetricTensor.load_from_dic(d, prefix="h")
+    su = SimpleUpdate.square_lattice_first_neighbor(h, int(d["D"]), float(d["tau"]),
+                                                    rcutoff=1e-10, degen_ratio=0.9999)
+    for k in range(2):
+        su.evolve(0.2)
+        assert abs(su.beta - float(d[f"b{k}_beta"])) < 1e-12
+        assert abs(su.logZ - float(d[f"b{k}_logZ"])) < 1e-11
+        for i, w in enumerate(su.get_weights()):
+            np.testing.assert_allclose(w, d[f"b{k}_w{i}"], rtol=1e-9, atol=1e-13)
+        for i, r in enumerate(su.get_bond_representations()):
+            assert np.array_equal(r, d[f"b{k}_rep{i}"])
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", su.get_tensors(), 20,
+                                                  cutoff=1e-10, degen_ratio=0.9999)
+    for it in range(3):
+        ctm.iterate()
+        assert np.array_equal(ctm.chi_values, d[f"it{it}_chi"])
+    for x, y in ctm.site_coords:
+        for kind, fn in (("rdm1x2", ctm.compute_rdm1x2), ("rdm2x1", ctm.compute_rdm2x1)):
+            got = fn(x, y).toarray()
+            assert np.abs(got - d[f"{kind}_{x}{y}"]).max() < 1e-8
+    assert abs(ctm.compute_PEPS_norm_log() - float(d["logZ_ctm"])) < 1e-8
