@@ -280,6 +280,13 @@ def heisenberg_u1():
     return U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
 
 
+def heisenberg_su2():
+    from frostspin_b200 import SU2SymmetricTensor
+
+    r = np.array([[1], [2]])
+    return SU2SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), (r, r), (r, r))
+
+
 def energy_per_bond(ctm):
     """Mean of tr(rho h) over the 4 inequivalent bonds of the AB/BA cell."""
     h = SDS_22.reshape(2, 2, 2, 2)
@@ -297,7 +304,8 @@ def ctmrg_setup(args):
     from frostspin_b200.simple_update import SimpleUpdate
 
     t0 = time.perf_counter()
-    su = SimpleUpdate.square_lattice_first_neighbor(heisenberg_u1(), args.D, 0.01,
+    h = heisenberg_su2() if args.symmetry == "su2" else heisenberg_u1()
+    su = SimpleUpdate.square_lattice_first_neighbor(h, args.D, 0.01,
                                                     rcutoff=1e-10, degen_ratio=0.9999)
     su.evolve(args.beta)
     tensors = su.get_tensors()
@@ -337,7 +345,7 @@ def timed_iterations(ctm, steps, precision, local):
 def run_ctmrg(args, world, rank, local):
     import torch
 
-    from frostspin_b200 import U1SymmetricTensor, linalg
+    from frostspin_b200 import linalg
 
     mixed = args.precision if args.precision != "fp64" else "ozaki6"
     su, tensors, ctm, t_su = ctmrg_setup(args)
@@ -370,7 +378,7 @@ def run_ctmrg(args, world, rank, local):
     ee = torch.cuda.Event(enable_timing=True)
     es.record()
     for _ in range(e2e_steps):
-        new = [U1SymmetricTensor.from_flat(t.row_reps, t.col_reps, h, t.block_irreps, t.signature)
+        new = [type(t).from_flat(t.row_reps, t.col_reps, h, t.block_irreps, t.signature)
                for t, h in zip(tensors, hostA, strict=True)]
         e2e_env.set_tensors(new)
         e2e_env.iterate()
@@ -418,8 +426,9 @@ def run_ctmrg(args, world, rank, local):
         "data": "synthetic (site tensors from the device simple update, seeded)",
         "impl": "ours",
         "config": {
-            "workload": "ctmrg_heisenberg_u1",
-            "model": "spin-1/2 Heisenberg square lattice, AB/BA cell, U(1) sectors",
+            "workload": f"ctmrg_heisenberg_{args.symmetry}",
+            "model": ("spin-1/2 Heisenberg square lattice, AB/BA cell, "
+                      + ("SU(2) multiplets" if args.symmetry == "su2" else "U(1) sectors")),
             "beta": args.beta, "D_target": args.D, "Dmax": su.Dmax, "chi": args.chi,
             "chi_values": [int(c) for c in ctm.chi_values],
             "precision": mixed if headline_mixed else "fp64",
@@ -443,7 +452,7 @@ def run_ctmrg(args, world, rank, local):
         "gpu_launches": lmx if headline_mixed else l64,
         "clocks": clkmx if headline_mixed else clk64,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.symmetry == "u1":
         t_cpu, info = cpu_ctmrg_seconds(tensors, ctm_mixed, args.chi)
         info["value"] = 1.0 / t_cpu
         info["unit"] = "iter/s"
@@ -737,8 +746,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["ctmrg", "u1_microbench"], default="ctmrg")
-    ap.add_argument("--D", type=int, default=12, help="simple-update bond dimension target")
-    ap.add_argument("--chi", type=int, default=64, help="CTMRG corner dimension target")
+    ap.add_argument("--symmetry", choices=["u1", "su2"], default="u1")
+    ap.add_argument("--D", type=int, default=None,
+                    help="simple-update bond dimension target (default 12 for U(1), 24 for SU(2))")
+    ap.add_argument("--chi", type=int, default=None,
+                    help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="ozaki6",
@@ -746,6 +758,10 @@ def main():
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
                     help="states per leg (256 = the benchmark; smaller for profiling)")
     args = ap.parse_args()
+    if args.D is None:
+        args.D = 24 if args.symmetry == "su2" else 12
+    if args.chi is None:
+        args.chi = 256 if args.symmetry == "su2" else 64
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

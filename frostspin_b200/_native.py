@@ -139,6 +139,8 @@ SIGNATURES = {
     ),
     "fs_dgemm_tile_shape": (ctypes.c_int, [_P, _P]),
     "fs_grouped_dgemm": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
+    "fs_thin_dgemm_shape": (ctypes.c_int, [_P, _P, _P]),
+    "fs_grouped_dgemm_thin": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
     "fs_ozaki_geometry": (ctypes.c_int, [_P, _P, _P, _P]),
     "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
@@ -194,7 +196,7 @@ CALL_COUNTS = {}
 
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
-    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1,
+    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
     "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1,
 }
@@ -221,3 +223,11 @@ def dgemm_tile_shape():
     tn = ctypes.c_int32()
     call("fs_dgemm_tile_shape", ctypes.byref(tm), ctypes.byref(tn))
     return tm.value, tn.value
+
+
+def thin_dgemm_shape():
+    mm = ctypes.c_int32()
+    mk = ctypes.c_int32()
+    tn = ctypes.c_int32()
+    call("fs_thin_dgemm_shape", ctypes.byref(mm), ctypes.byref(mk), ctypes.byref(tn))
+    return mm.value, mk.value, tn.value

@@ -1,12 +1,20 @@
-// Grouped FP64 GEMM over irrep sectors: the plain double-precision path.
+// Grouped FP64 GEMM over irrep sectors: the plain double-precision path, on the
+// FP64 tensor cores (DMMA, mma.sync m8n8k4 f64 -- Blackwell has no tcgen05 kind
+// for f64, so this is the FP64 tensor path of sm_100a).
 //
 // Reference behaviour: SymmetricTensor.__matmul__ (frostspin/symmetric_tensor/
 // symmetric_tensor.py:453-489) calls numpy's dgemm once per shared irrep block.
 // Here every sector product of one contraction is a problem in one launch; the
 // host flattens all output tiles of all problems into a tile list and CTAs
 // stride over it (a static persistent schedule), so sectors of very uneven
-// sizes share the machine.  64x64 output tile, 16-deep k slices staged through
-// shared memory with register double buffering, 4x4 outputs per thread.
+// sizes share the machine.
+//
+// 64x64 output tile per CTA, 4 warps of 32x32 (4x4 m8n8 fragments), k staged
+// 16 deep through a 4-stage cp.async pipeline.  Sector blocks start at any
+// element offset, so copies are 8-byte cp.async with zero fill at the edges.
+// Shared layouts follow the global layout of each operand (row- or
+// column-major, per problem) with padding chosen so that every fragment load
+// of a half warp touches 32 distinct banks.
 #include "common.cuh"
 
 namespace fsb {
@@ -14,99 +22,90 @@ namespace fsb {
 constexpr int kTM = 64;
 constexpr int kTN = 64;
 constexpr int kTK = 16;
-constexpr int kGemmThreads = 256;
+constexpr int kStages = 4;
+constexpr int kGemmThreads = 128;
+constexpr int kLdK = kTK + 4;   // stride of a [row][k] tile (20 doubles, 4 mod 16)
+constexpr int kLdR = kTM + 4;   // stride of a [k][row] tile (68 doubles, 4 mod 16)
+constexpr int kOpTile = kTM * kLdK;  // >= kTK * kLdR
+static_assert(kTM == kTN, "square tiles: one stage size for A and B");
+static_assert(kOpTile >= kTK * kLdR, "stage too small for the k-major layout");
+constexpr int kStageDoubles = 2 * kOpTile;
+constexpr size_t kGemmSmem = sizeof(double) * kStageDoubles * kStages;
 
-struct __align__(16) GemmSmem {
-    double a[2][kTK][kTM + 2];
-    double b[2][kTK][kTN + 2];
-};
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    const int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n));
+}
 
-__device__ __forceinline__ void load_a_regs(const FsGemmProblem& p, int m0, int k0,
-                                            double (&r)[4]) {
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::);
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+// One k slice of op(A) (rows m0.., k0..) and op(B) (k0.., cols n0..) into a stage.
+// A stage holds A in [m][k] (transA == 0) or [k][m] (transA == 1) and B in
+// [k][n] (transB == 0) or [n][k] (transB == 1): always the global contiguous
+// direction innermost, so the copies are coalesced.
+__device__ __forceinline__ void load_stage(const FsGemmProblem& p, int m0, int n0, int k0,
+                                           double* stage) {
+    double* sa = stage;
+    double* sb = stage + kOpTile;
+    const double* A = p.A;
+    const double* B = p.B;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int idx = threadIdx.x + u * kGemmThreads;
-        int i, k;
+    for (int u = 0; u < (kTM * kTK) / kGemmThreads; ++u) {
+        const int e = threadIdx.x + u * kGemmThreads;
         if (p.transA) {
-            k = idx / kTM;
-            i = idx % kTM;
+            const int k = e / kTM, m = e % kTM;
+            const bool ok = (m0 + m < p.M) && (k0 + k < p.K);
+            const double* src = ok ? A + static_cast<int64_t>(k0 + k) * p.lda + (m0 + m) : A;
+            cp_async8(sa + k * kLdR + m, src, ok);
         } else {
-            i = idx / kTK;
-            k = idx % kTK;
+            const int m = e / kTK, k = e % kTK;
+            const bool ok = (m0 + m < p.M) && (k0 + k < p.K);
+            const double* src = ok ? A + static_cast<int64_t>(m0 + m) * p.lda + (k0 + k) : A;
+            cp_async8(sa + m * kLdK + k, src, ok);
         }
-        const int gi = m0 + i, gk = k0 + k;
-        double v = 0.0;
-        if (gi < p.M && gk < p.K) {
-            v = p.transA ? __ldg(p.A + static_cast<int64_t>(gk) * p.lda + gi)
-                         : __ldg(p.A + static_cast<int64_t>(gi) * p.lda + gk);
-        }
-        r[u] = v;
     }
-}
-
-__device__ __forceinline__ void store_a_smem(const FsGemmProblem& p, double (*sa)[kTM + 2],
-                                             const double (&r)[4]) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int idx = threadIdx.x + u * kGemmThreads;
-        int i, k;
-        if (p.transA) {
-            k = idx / kTM;
-            i = idx % kTM;
-        } else {
-            i = idx / kTK;
-            k = idx % kTK;
-        }
-        sa[k][i] = r[u];
-    }
-}
-
-__device__ __forceinline__ void load_b_regs(const FsGemmProblem& p, int n0, int k0,
-                                            double (&r)[4]) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int idx = threadIdx.x + u * kGemmThreads;
-        int j, k;
+    for (int u = 0; u < (kTN * kTK) / kGemmThreads; ++u) {
+        const int e = threadIdx.x + u * kGemmThreads;
         if (p.transB) {
-            j = idx / kTK;
-            k = idx % kTK;
+            const int n = e / kTK, k = e % kTK;
+            const bool ok = (n0 + n < p.N) && (k0 + k < p.K);
+            const double* src = ok ? B + static_cast<int64_t>(n0 + n) * p.ldb + (k0 + k) : B;
+            cp_async8(sb + n * kLdK + k, src, ok);
         } else {
-            k = idx / kTN;
-            j = idx % kTN;
+            const int k = e / kTN, n = e % kTN;
+            const bool ok = (n0 + n < p.N) && (k0 + k < p.K);
+            const double* src = ok ? B + static_cast<int64_t>(k0 + k) * p.ldb + (n0 + n) : B;
+            cp_async8(sb + k * kLdR + n, src, ok);
         }
-        const int gj = n0 + j, gk = k0 + k;
-        double v = 0.0;
-        if (gj < p.N && gk < p.K) {
-            v = p.transB ? __ldg(p.B + static_cast<int64_t>(gj) * p.ldb + gk)
-                         : __ldg(p.B + static_cast<int64_t>(gk) * p.ldb + gj);
-        }
-        r[u] = v;
-    }
-}
-
-__device__ __forceinline__ void store_b_smem(const FsGemmProblem& p, double (*sb)[kTN + 2],
-                                             const double (&r)[4]) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int idx = threadIdx.x + u * kGemmThreads;
-        int j, k;
-        if (p.transB) {
-            j = idx / kTK;
-            k = idx % kTK;
-        } else {
-            k = idx / kTN;
-            j = idx % kTN;
-        }
-        sb[k][j] = r[u];
     }
 }
 
 __global__ void __launch_bounds__(kGemmThreads)
     k_grouped_dgemm(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
                     const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
-    __shared__ GemmSmem sm;
-    const int tx = threadIdx.x % 16;
-    const int ty = threadIdx.x / 16;
+    extern __shared__ __align__(16) double smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wm = (warp & 1) * 32;
+    const int wn = (warp >> 1) * 32;
+    const int fr = lane >> 2;  // fragment row (A, C) / column (B)
+    const int fk = lane & 3;   // fragment k (A, B) / column pair (C)
+
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const FsGemmTile tile = tiles[t];
         if (tile.problem < 0 || tile.problem >= n_problems) continue;
@@ -115,60 +114,65 @@ __global__ void __launch_bounds__(kGemmThreads)
         const int n0 = tile.tn * kTN;
         if (m0 >= p.M || n0 >= p.N) continue;
 
-        double acc[4][4];
+        double acc[4][4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-        double ra[4], rb[4];
         const int nk = (p.K + kTK - 1) / kTK;
-        __syncthreads();  // previous tile finished reading smem
-        if (nk > 0) {
-            load_a_regs(p, m0, 0, ra);
-            load_b_regs(p, n0, 0, rb);
-            store_a_smem(p, sm.a[0], ra);
-            store_b_smem(p, sm.b[0], rb);
-        }
-        __syncthreads();
-        for (int kt = 0; kt < nk; ++kt) {
-            const int cur = kt & 1;
-            if (kt + 1 < nk) {
-                load_a_regs(p, m0, (kt + 1) * kTK, ra);
-                load_b_regs(p, n0, (kt + 1) * kTK, rb);
-            }
+        __syncthreads();  // every warp is done with the previous tile's stages
 #pragma unroll
-            for (int k = 0; k < kTK; ++k) {
-                double av[4], bv[4];
-                const double2 a01 = *reinterpret_cast<const double2*>(&sm.a[cur][k][ty * 4]);
-                const double2 a23 = *reinterpret_cast<const double2*>(&sm.a[cur][k][ty * 4 + 2]);
-                const double2 b01 = *reinterpret_cast<const double2*>(&sm.b[cur][k][tx * 4]);
-                const double2 b23 = *reinterpret_cast<const double2*>(&sm.b[cur][k][tx * 4 + 2]);
-                av[0] = a01.x; av[1] = a01.y; av[2] = a23.x; av[3] = a23.y;
-                bv[0] = b01.x; bv[1] = b01.y; bv[2] = b23.x; bv[3] = b23.y;
+        for (int s = 0; s < kStages - 1; ++s) {
+            if (s < nk) load_stage(p, m0, n0, s * kTK, smem + s * kStageDoubles);
+            cp_async_commit();
+        }
+        for (int kt = 0; kt < nk; ++kt) {
+            cp_async_wait<kStages - 2>();
+            __syncthreads();
+            {
+                const int nxt = kt + kStages - 1;
+                if (nxt < nk)
+                    load_stage(p, m0, n0, nxt * kTK, smem + (nxt % kStages) * kStageDoubles);
+                cp_async_commit();
+            }
+            const double* sa = smem + (kt % kStages) * kStageDoubles;
+            const double* sb = sa + kOpTile;
+#pragma unroll
+            for (int kk = 0; kk < kTK; kk += 4) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int m = wm + i * 8 + fr;
+                    a[i] = p.transA ? sa[(kk + fk) * kLdR + m] : sa[m * kLdK + kk + fk];
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int n = wn + j * 8 + fr;
+                    b[j] = p.transB ? sb[n * kLdK + kk + fk] : sb[(kk + fk) * kLdR + n];
+                }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                    for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
             }
-            if (kt + 1 < nk) {
-                store_a_smem(p, sm.a[cur ^ 1], ra);
-                store_b_smem(p, sm.b[cur ^ 1], rb);
-            }
-            __syncthreads();
         }
+        cp_async_wait<0>();
 
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int gi = m0 + ty * 4 + i;
+            const int gi = m0 + wm + i * 8 + fr;
             if (gi >= p.M) continue;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int gj = n0 + tx * 4 + j;
-                if (gj >= p.N) continue;
-                double* c = p.C + static_cast<int64_t>(gi) * p.ldc + gj;
-                const double v = p.alpha * acc[i][j];
-                *c = (p.beta == 0.0) ? v : fma(p.beta, *c, v);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int gj = n0 + wn + j * 8 + fk * 2 + h;
+                    if (gj >= p.N) continue;
+                    double* c = p.C + static_cast<int64_t>(gi) * p.ldc + gj;
+                    const double v = p.alpha * acc[i][j][h];
+                    *c = (p.beta == 0.0) ? v : fma(p.beta, *c, v);
+                }
             }
         }
     }
@@ -188,9 +192,119 @@ extern "C" int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_probl
     if (n_tiles < 0 || n_problems < 0) return FS_ERR_INVALID_ARG;
     if (n_tiles == 0) return FS_OK;
     if (d_problems == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 4;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(fsb::k_grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(fsb::kGemmSmem)) != cudaSuccess)
+            return fsb::launch_status();
+        configured = true;
+    }
+    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 2;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
-    fsb::k_grouped_dgemm<<<grid, fsb::kGemmThreads, 0, fsb::as_stream(stream)>>>(
+    fsb::k_grouped_dgemm<<<grid, fsb::kGemmThreads, fsb::kGemmSmem, fsb::as_stream(stream)>>>(
+        d_problems, n_problems, d_tiles, n_tiles);
+    return fsb::launch_status();
+}
+
+// ---------------------------------------------------------------- thin GEMMs
+// C[MxN] = alpha A[MxK] B[KxN] + beta C for M, K <= 32 and N large: the
+// recoupling products of a non-abelian permute (one small isometry applied to
+// many external-degeneracy columns).  Bandwidth bound: each thread owns output
+// columns, A is staged once per tile in shared memory and read as broadcasts,
+// the accumulators live in registers (M rounded up to 4, 8, 16 or 32).  Both
+// operands row-major (transA == transB == 0; the host checks).
+namespace fsb {
+
+constexpr int kThinMax = 32;
+constexpr int kThinThreads = 128;
+constexpr int kThinColsPerThread = 2;
+
+template <int MB>
+__device__ __forceinline__ void thin_tile(const FsGemmProblem& p, const double* su, int n0) {
+    double acc[kThinColsPerThread][MB];
+#pragma unroll
+    for (int c = 0; c < kThinColsPerThread; ++c)
+#pragma unroll
+        for (int m = 0; m < MB; ++m) acc[c][m] = 0.0;
+    int cols[kThinColsPerThread];
+    bool ok[kThinColsPerThread];
+#pragma unroll
+    for (int c = 0; c < kThinColsPerThread; ++c) {
+        cols[c] = n0 + threadIdx.x + c * kThinThreads;
+        ok[c] = cols[c] < p.N;
+    }
+    for (int k = 0; k < p.K; ++k) {
+        double x[kThinColsPerThread];
+#pragma unroll
+        for (int c = 0; c < kThinColsPerThread; ++c)
+            x[c] = ok[c] ? __ldg(p.B + static_cast<int64_t>(k) * p.ldb + cols[c]) : 0.0;
+#pragma unroll
+        for (int m = 0; m < MB; ++m) {
+            const double u = su[m * kThinMax + k];
+#pragma unroll
+            for (int c = 0; c < kThinColsPerThread; ++c) acc[c][m] = fma(u, x[c], acc[c][m]);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < MB; ++m) {
+        if (m >= p.M) break;
+#pragma unroll
+        for (int c = 0; c < kThinColsPerThread; ++c) {
+            if (!ok[c]) continue;
+            double* dst = p.C + static_cast<int64_t>(m) * p.ldc + cols[c];
+            const double v = p.alpha * acc[c][m];
+            *dst = (p.beta == 0.0) ? v : fma(p.beta, *dst, v);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThinThreads)
+    k_grouped_dgemm_thin(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
+                         const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
+    __shared__ double su[kThinMax * kThinMax];
+    constexpr int kCols = kThinThreads * kThinColsPerThread;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const FsGemmTile tile = tiles[t];
+        if (tile.problem < 0 || tile.problem >= n_problems) continue;
+        const FsGemmProblem p = problems[tile.problem];
+        if (p.M > kThinMax || p.K > kThinMax || p.transA || p.transB) continue;
+        const int n0 = tile.tn * kCols;
+        if (n0 >= p.N) continue;
+        __syncthreads();  // previous tile's reads of su are done
+        for (int i = threadIdx.x; i < kThinMax * kThinMax; i += kThinThreads) {
+            const int m = i / kThinMax, k = i % kThinMax;
+            su[i] = (m < p.M && k < p.K) ? p.A[static_cast<int64_t>(m) * p.lda + k] : 0.0;
+        }
+        __syncthreads();
+        if (p.M <= 4)
+            thin_tile<4>(p, su, n0);
+        else if (p.M <= 8)
+            thin_tile<8>(p, su, n0);
+        else if (p.M <= 16)
+            thin_tile<16>(p, su, n0);
+        else
+            thin_tile<32>(p, su, n0);
+    }
+}
+
+}  // namespace fsb
+
+extern "C" int fs_thin_dgemm_shape(int32_t* max_m, int32_t* max_k, int32_t* tile_n) {
+    if (max_m == nullptr || max_k == nullptr || tile_n == nullptr) return FS_ERR_INVALID_ARG;
+    *max_m = fsb::kThinMax;
+    *max_k = fsb::kThinMax;
+    *tile_n = fsb::kThinThreads * fsb::kThinColsPerThread;
+    return FS_OK;
+}
+
+extern "C" int fs_grouped_dgemm_thin(const FsGemmProblem* d_problems, int64_t n_problems,
+                                     const FsGemmTile* d_tiles, int64_t n_tiles, void* stream) {
+    if (n_tiles < 0 || n_problems < 0) return FS_ERR_INVALID_ARG;
+    if (n_tiles == 0) return FS_OK;
+    if (d_problems == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 8;
+    const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
+    fsb::k_grouped_dgemm_thin<<<grid, fsb::kThinThreads, 0, fsb::as_stream(stream)>>>(
         d_problems, n_problems, d_tiles, n_tiles);
     return fsb::launch_status();
 }

@@ -16,7 +16,7 @@ from . import instrument
 
 # ----------------------------------------------------------------- precision
 
-_PRECISION = {"gemm": "fp64"}
+_PRECISION = {"gemm": "fp64", "dispatch": "cost"}
 PRECISIONS = ("fp64",) + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
 
 
@@ -43,6 +43,20 @@ def gemm_precision_mode(mode):
         yield
     finally:
         set_gemm_precision(old)
+
+
+@contextlib.contextmanager
+def ozaki_dispatch_mode(kind):
+    """Which sector GEMMs take the Ozaki path in an ozakiS mode: "cost" (the
+    default: those the cost model finds faster than FP64) or "all"."""
+    if kind not in ("cost", "all"):
+        raise ValueError(kind)
+    old = _PRECISION["dispatch"]
+    _PRECISION["dispatch"] = kind
+    try:
+        yield
+    finally:
+        _PRECISION["dispatch"] = old
 
 
 # ------------------------------------------------------------- grouped GEMM
@@ -93,7 +107,10 @@ def grouped_gemm(problems):
             _dgemm(arr, problems, tm, tn, ntile)
     elif mode.startswith("ozaki"):
         S = int(mode[5:])
-        use = ozaki_pays(arr, S)
+        if _PRECISION["dispatch"] == "all":
+            use = np.ones(arr.size, dtype=bool)
+        else:
+            use = ozaki_pays(arr, S)
         if use.any():
             with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
                                    int8_ops=ozaki_int8_ops(arr[use], S)):
@@ -105,18 +122,49 @@ def grouped_gemm(problems):
         raise ValueError(mode)
 
 
+_THIN = None
+
+
+def _thin_shape():
+    global _THIN
+    if _THIN is None:
+        _THIN = _native.thin_dgemm_shape()
+    return _THIN
+
+
 def grouped_dgemm_table(arr, region="gemm_fp64"):
     """FP64 grouped GEMM over a prepared FsGemmProblem table (pointers already
-    set); always FP64, whatever the precision mode."""
+    set); always FP64, whatever the precision mode.  Thin row-major problems
+    (M, K <= 32) go to the bandwidth kernel, the rest to the DMMA kernel."""
     if arr.size == 0:
         return
-    tm, tn = _tile_shape()
+    max_m, max_k, thin_n = _thin_shape()
     M = arr["M"].astype(np.int64)
     N = arr["N"].astype(np.int64)
-    ntile = ((M + tm - 1) // tm) * ((N + tn - 1) // tn)
-    flops = 2.0 * float((M.astype(np.float64) * N * arr["K"]).sum())
-    with instrument.region(region, flops=flops):
-        _dgemm(arr, None, tm, tn, ntile)
+    K = arr["K"].astype(np.int64)
+    thin = (M <= max_m) & (K <= max_k) & (arr["transA"] == 0) & (arr["transB"] == 0)
+    if thin.any():
+        sub = arr[thin]
+        nt = (N[thin] + thin_n - 1) // thin_n
+        total = int(nt.sum())
+        tiles = np.zeros(total, dtype=_native.GEMM_TILE_DTYPE)
+        pid = np.repeat(np.arange(sub.size), nt)
+        tiles["problem"] = pid
+        tiles["tn"] = np.arange(total) - np.repeat(np.cumsum(nt) - nt, nt)
+        d_prob = dev.upload(sub)
+        d_tiles = dev.upload(tiles)
+        flops = 2.0 * float((M[thin].astype(np.float64) * N[thin] * K[thin]).sum())
+        with instrument.region(region + "_thin", flops=flops,
+                               bytes=8.0 * float((N[thin] * (M[thin] + K[thin])).sum())):
+            _native.call("fs_grouped_dgemm_thin", d_prob.data_ptr(), sub.size,
+                         d_tiles.data_ptr(), total, dev.stream())
+    if (~thin).any():
+        sub = arr[~thin]
+        tm, tn = _tile_shape()
+        ntile = ((M[~thin] + tm - 1) // tm) * ((N[~thin] + tn - 1) // tn)
+        flops = 2.0 * float((M[~thin].astype(np.float64) * N[~thin] * K[~thin]).sum())
+        with instrument.region(region, flops=flops):
+            _dgemm(sub, None, tm, tn, ntile)
 
 
 # rough rates of the two paths on B200 (measured on the U(1) microbench), used

@@ -134,6 +134,18 @@ int fs_dgemm_tile_shape(int32_t* tile_m, int32_t* tile_n);
 int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_problems,
                      const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
 
+/*
+ * Thin problems of the same table format: M <= max_m, K <= max_k, both
+ * operands row-major (transA == transB == 0), N large -- the recoupling
+ * products of the SU(2) permute (frostspin/symmetric_tensor/
+ * lie_group_symmetric_tensor.py:179, new += U_sector @ old).  Tiles are
+ * (problem, tn) over tile_n columns (tm unused).  Problems outside those
+ * limits are skipped; the host routes them to fs_grouped_dgemm.
+ */
+int fs_thin_dgemm_shape(int32_t* max_m, int32_t* max_k, int32_t* tile_n);
+int fs_grouped_dgemm_thin(const FsGemmProblem* d_problems, int64_t n_problems,
+                          const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
+
 /* ------------------------------------- grouped GEMM on tcgen05 (Ozaki int8) */
 /*
  * FP64-class GEMM on the int8 tensor cores (tcgen05.mma kind::i8): every row of

@@ -1,0 +1,62 @@
+"""FP64 grouped GEMM kernels (DMMA tiles and the thin bandwidth kernel) against
+a numpy float64 reference: every transpose combination, ragged edges, K = 0,
+beta != 0 and thin recoupling shapes, all problems of a table in one launch."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [  # (M, N, K)
+    (1, 1, 1), (7, 5, 3), (64, 64, 16), (65, 63, 17), (130, 257, 129), (3, 1000, 2),
+    (32, 4097, 32), (4, 20000, 4), (33, 300, 31), (200, 3, 500), (16, 16, 0), (1, 517, 29),
+]
+
+
+def run_table(problems, trans_a, trans_b, beta):
+    import torch
+
+    from frostspin_b200 import _native, linalg
+
+    rng = np.random.default_rng(17)
+    arr = np.zeros(len(problems), dtype=_native.GEMM_PROBLEM_DTYPE)
+    keep, refs, outs = [], [], []
+    for i, (M, N, K) in enumerate(problems):
+        A = rng.standard_normal((M, K))
+        B = rng.standard_normal((K, N))
+        C0 = rng.standard_normal((M, N))
+        dA = torch.from_numpy(np.ascontiguousarray(A.T if trans_a else A)).cuda()
+        dB = torch.from_numpy(np.ascontiguousarray(B.T if trans_b else B)).cuda()
+        dC = torch.from_numpy(C0.copy()).cuda()
+        keep += [dA, dB]
+        outs.append(dC)
+        refs.append((A @ B * 1.5 + beta * C0,
+                     np.abs(A).sum(axis=1)[:, None] * np.abs(B).max(initial=0.0)))
+        arr[i] = (dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M if trans_a else K,
+                  K if trans_b else N, N, M, N, K, int(trans_a), int(trans_b), 0, 1.5, beta)
+    linalg.grouped_dgemm_table(arr)
+    torch.cuda.synchronize()
+    for (ref, scale), dC in zip(refs, outs, strict=True):
+        got = dC.cpu().numpy()
+        assert np.all(np.abs(got - ref) <= 1e-14 * (scale + 1.0) * 4 + 1e-15)
+
+
+@pytest.mark.parametrize("trans_a", [False, True])
+@pytest.mark.parametrize("trans_b", [False, True])
+def test_grouped_dgemm_all_layouts(trans_a, trans_b):
+    run_table(SHAPES, trans_a, trans_b, 0.0)
+
+
+def test_grouped_dgemm_beta_accumulates():
+    run_table(SHAPES, False, False, 0.75)
+    run_table(SHAPES[:6], True, False, -2.0)
+
+
+def test_thin_and_tile_kernels_both_launch():
+    from frostspin_b200 import _native
+
+    before = dict(_native.CALL_COUNTS)
+    run_table([(4, 5000, 4), (100, 100, 100)], False, False, 0.0)
+    after = _native.CALL_COUNTS
+    assert after.get("fs_grouped_dgemm_thin", 0) - before.get("fs_grouped_dgemm_thin", 0) == 1
+    assert after.get("fs_grouped_dgemm", 0) - before.get("fs_grouped_dgemm", 0) == 1

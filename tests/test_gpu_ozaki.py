@@ -50,7 +50,7 @@ def run_grouped(problems, mode):
                       "C": C.reshape(-1), "c_off": 0,
                       "M": A.shape[0], "N": B.shape[1], "K": A.shape[1],
                       "_keep": (dA, dB)})
-    with linalg.gemm_precision_mode(mode):
+    with linalg.gemm_precision_mode(mode), linalg.ozaki_dispatch_mode("all"):
         linalg.grouped_gemm(specs)
     torch.cuda.synchronize()
     linalg.check_ozaki_flags()
