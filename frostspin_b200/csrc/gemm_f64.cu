@@ -10,11 +10,12 @@
 // sizes share the machine.
 //
 // 64x64 output tile per CTA, 4 warps of 32x32 (4x4 m8n8 fragments), k staged
-// 16 deep through a 4-stage cp.async pipeline.  Sector blocks start at any
-// element offset, so copies are 8-byte cp.async with zero fill at the edges.
-// Shared layouts follow the global layout of each operand (row- or
-// column-major, per problem) with padding chosen so that every fragment load
-// of a half warp touches 32 distinct banks.
+// 16 deep through a 3-stage cp.async pipeline, 3 CTAs per SM.  Sector blocks
+// start at any element offset, so copies are 8-byte cp.async with zero fill at
+// the edges.  Shared layouts follow the global layout of each operand (row- or
+// column-major, per problem; the tile body is instantiated for the four
+// combinations) with padding chosen so that every fragment load of a half warp
+// touches 32 distinct banks.
 #include "common.cuh"
 
 namespace fsb {
@@ -22,7 +23,7 @@ namespace fsb {
 constexpr int kTM = 64;
 constexpr int kTN = 64;
 constexpr int kTK = 16;
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kGemmThreads = 128;
 constexpr int kLdK = kTK + 4;   // stride of a [row][k] tile (20 doubles, 4 mod 16)
 constexpr int kLdR = kTM + 4;   // stride of a [k][row] tile (68 doubles, 4 mod 16)
@@ -54,51 +55,40 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
 }
 
 // One k slice of op(A) (rows m0.., k0..) and op(B) (k0.., cols n0..) into a stage.
-// A stage holds A in [m][k] (transA == 0) or [k][m] (transA == 1) and B in
-// [k][n] (transB == 0) or [n][k] (transB == 1): always the global contiguous
-// direction innermost, so the copies are coalesced.
+// A stage holds A in [m][k] (TA == 0) or [k][m] (TA == 1) and B in [k][n]
+// (TB == 0) or [n][k] (TB == 1): always the global contiguous direction
+// innermost, so the copies are coalesced.
+template <bool TA, bool TB>
 __device__ __forceinline__ void load_stage(const FsGemmProblem& p, int m0, int n0, int k0,
                                            double* stage) {
     double* sa = stage;
     double* sb = stage + kOpTile;
-    const double* A = p.A;
-    const double* B = p.B;
 #pragma unroll
     for (int u = 0; u < (kTM * kTK) / kGemmThreads; ++u) {
         const int e = threadIdx.x + u * kGemmThreads;
-        if (p.transA) {
-            const int k = e / kTM, m = e % kTM;
-            const bool ok = (m0 + m < p.M) && (k0 + k < p.K);
-            const double* src = ok ? A + static_cast<int64_t>(k0 + k) * p.lda + (m0 + m) : A;
-            cp_async8(sa + k * kLdR + m, src, ok);
-        } else {
-            const int m = e / kTK, k = e % kTK;
-            const bool ok = (m0 + m < p.M) && (k0 + k < p.K);
-            const double* src = ok ? A + static_cast<int64_t>(m0 + m) * p.lda + (k0 + k) : A;
-            cp_async8(sa + m * kLdK + k, src, ok);
-        }
+        const int k = TA ? e / kTM : e % kTK;
+        const int m = TA ? e % kTM : e / kTK;
+        const bool ok = (m0 + m < p.M) && (k0 + k < p.K);
+        const int64_t off = TA ? static_cast<int64_t>(k0 + k) * p.lda + (m0 + m)
+                               : static_cast<int64_t>(m0 + m) * p.lda + (k0 + k);
+        cp_async8(sa + (TA ? k * kLdR + m : m * kLdK + k), ok ? p.A + off : p.A, ok);
     }
 #pragma unroll
     for (int u = 0; u < (kTN * kTK) / kGemmThreads; ++u) {
         const int e = threadIdx.x + u * kGemmThreads;
-        if (p.transB) {
-            const int n = e / kTK, k = e % kTK;
-            const bool ok = (n0 + n < p.N) && (k0 + k < p.K);
-            const double* src = ok ? B + static_cast<int64_t>(n0 + n) * p.ldb + (k0 + k) : B;
-            cp_async8(sb + n * kLdK + k, src, ok);
-        } else {
-            const int k = e / kTN, n = e % kTN;
-            const bool ok = (n0 + n < p.N) && (k0 + k < p.K);
-            const double* src = ok ? B + static_cast<int64_t>(k0 + k) * p.ldb + (n0 + n) : B;
-            cp_async8(sb + k * kLdR + n, src, ok);
-        }
+        const int k = TB ? e % kTK : e / kTN;
+        const int n = TB ? e / kTK : e % kTN;
+        const bool ok = (n0 + n < p.N) && (k0 + k < p.K);
+        const int64_t off = TB ? static_cast<int64_t>(n0 + n) * p.ldb + (k0 + k)
+                               : static_cast<int64_t>(k0 + k) * p.ldb + (n0 + n);
+        cp_async8(sb + (TB ? n * kLdK + k : k * kLdR + n), ok ? p.B + off : p.B, ok);
     }
 }
 
-__global__ void __launch_bounds__(kGemmThreads)
-    k_grouped_dgemm(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
-                    const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
-    extern __shared__ __align__(16) double smem[];
+// One 64x64 output tile: the cp.async pipeline over k and the DMMA fragments.
+template <bool TA, bool TB>
+__device__ __forceinline__ void dgemm_tile(const FsGemmProblem& p, int m0, int n0,
+                                           double* smem) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int wm = (warp & 1) * 32;
@@ -106,6 +96,75 @@ __global__ void __launch_bounds__(kGemmThreads)
     const int fr = lane >> 2;  // fragment row (A, C) / column (B)
     const int fk = lane & 3;   // fragment k (A, B) / column pair (C)
 
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    // per-thread fragment offsets inside a stage (k = 0)
+    const int a_off = TA ? fk * kLdR + wm + fr : (wm + fr) * kLdK + fk;
+    const int b_off = TB ? (wn + fr) * kLdK + fk : fk * kLdR + wn + fr;
+    constexpr int a_step_i = TA ? 8 : 8 * kLdK;   // next fragment row block
+    constexpr int a_step_k = TA ? 4 * kLdR : 4;   // next k-step
+    constexpr int b_step_j = TB ? 8 * kLdK : 8;
+    constexpr int b_step_k = TB ? 4 : 4 * kLdR;
+
+    const int nk = (p.K + kTK - 1) / kTK;
+    __syncthreads();  // every warp is done with the previous tile's stages
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load_stage<TA, TB>(p, m0, n0, s * kTK, smem + s * kStageDoubles);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        {
+            const int nxt = kt + kStages - 1;
+            if (nxt < nk)
+                load_stage<TA, TB>(p, m0, n0, nxt * kTK, smem + (nxt % kStages) * kStageDoubles);
+            cp_async_commit();
+        }
+        const double* sa = smem + (kt % kStages) * kStageDoubles + a_off;
+        const double* sb = smem + (kt % kStages) * kStageDoubles + kOpTile + b_off;
+#pragma unroll
+        for (int ks = 0; ks < kTK / 4; ++ks) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sa[ks * a_step_k + i * a_step_i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sb[ks * b_step_k + j * b_step_j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
+        }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gi = m0 + wm + i * 8 + fr;
+        if (gi >= p.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = n0 + wn + j * 8 + fk * 2 + h;
+                if (gj >= p.N) continue;
+                double* c = p.C + static_cast<int64_t>(gi) * p.ldc + gj;
+                const double v = p.alpha * acc[i][j][h];
+                *c = (p.beta == 0.0) ? v : fma(p.beta, *c, v);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 3)
+    k_grouped_dgemm(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
+                    const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
+    extern __shared__ __align__(16) double smem[];
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const FsGemmTile tile = tiles[t];
         if (tile.problem < 0 || tile.problem >= n_problems) continue;
@@ -113,67 +172,11 @@ __global__ void __launch_bounds__(kGemmThreads)
         const int m0 = tile.tm * kTM;
         const int n0 = tile.tn * kTN;
         if (m0 >= p.M || n0 >= p.N) continue;
-
-        double acc[4][4][2];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-        const int nk = (p.K + kTK - 1) / kTK;
-        __syncthreads();  // every warp is done with the previous tile's stages
-#pragma unroll
-        for (int s = 0; s < kStages - 1; ++s) {
-            if (s < nk) load_stage(p, m0, n0, s * kTK, smem + s * kStageDoubles);
-            cp_async_commit();
-        }
-        for (int kt = 0; kt < nk; ++kt) {
-            cp_async_wait<kStages - 2>();
-            __syncthreads();
-            {
-                const int nxt = kt + kStages - 1;
-                if (nxt < nk)
-                    load_stage(p, m0, n0, nxt * kTK, smem + (nxt % kStages) * kStageDoubles);
-                cp_async_commit();
-            }
-            const double* sa = smem + (kt % kStages) * kStageDoubles;
-            const double* sb = sa + kOpTile;
-#pragma unroll
-            for (int kk = 0; kk < kTK; kk += 4) {
-                double a[4], b[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int m = wm + i * 8 + fr;
-                    a[i] = p.transA ? sa[(kk + fk) * kLdR + m] : sa[m * kLdK + kk + fk];
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int n = wn + j * 8 + fr;
-                    b[j] = p.transB ? sb[n * kLdK + kk + fk] : sb[(kk + fk) * kLdR + n];
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
-            }
-        }
-        cp_async_wait<0>();
-
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int gi = m0 + wm + i * 8 + fr;
-            if (gi >= p.M) continue;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int gj = n0 + wn + j * 8 + fk * 2 + h;
-                    if (gj >= p.N) continue;
-                    double* c = p.C + static_cast<int64_t>(gi) * p.ldc + gj;
-                    const double v = p.alpha * acc[i][j][h];
-                    *c = (p.beta == 0.0) ? v : fma(p.beta, *c, v);
-                }
-            }
+        switch ((p.transA ? 2 : 0) | (p.transB ? 1 : 0)) {
+            case 0: dgemm_tile<false, false>(p, m0, n0, smem); break;
+            case 1: dgemm_tile<false, true>(p, m0, n0, smem); break;
+            case 2: dgemm_tile<true, false>(p, m0, n0, smem); break;
+            default: dgemm_tile<true, true>(p, m0, n0, smem); break;
         }
     }
 }
@@ -199,7 +202,7 @@ extern "C" int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_probl
             return fsb::launch_status();
         configured = true;
     }
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 2;
+    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 3;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
     fsb::k_grouped_dgemm<<<grid, fsb::kGemmThreads, fsb::kGemmSmem, fsb::as_stream(stream)>>>(
         d_problems, n_problems, d_tiles, n_tiles);

@@ -424,24 +424,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) +
                                            acc * kTileN;
                     const int shift = -7 * (d + 2);
+                    // C is read only when it contributes (later diagonals, or
+                    // beta != 0), and the 16 reads of a chunk are issued before
+                    // any store so that they overlap instead of each waiting a
+                    // full memory latency behind the previous store
+                    const bool read_c = !first || p.beta != 0.0;
                     for (int cb = 0; cb < kTileN; cb += 16) {
                         uint32_t v[16];
                         tmem_ld16(taddr + cb, v);
-                        if (!row_ok) continue;
-                        double* crow = p.C + row * p.ldc;
+                        if (!row_ok || col0 + cb >= p.N) continue;
+                        double* crow = p.C + row * p.ldc + col0 + cb;
+                        const int32_t* be = p.b_exps + col0 + cb;
+                        const int ncol = min(16, p.N - col0 - cb);
+                        double old[16];
+                        int eb[16];
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
-                            const int col = col0 + cb + j;
-                            if (col >= p.N) continue;
+                            eb[j] = (j < ncol) ? __ldg(be + j) : 0;
+                            old[j] = (read_c && j < ncol) ? crow[j] : 0.0;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
                             const double val =
                                 p.alpha * ldexp(static_cast<double>(static_cast<int32_t>(v[j])),
-                                                ea + p.b_exps[col] + shift);
-                            if (first) {
-                                crow[col] = (p.beta == 0.0) ? val : fma(p.beta, crow[col], val);
-                            } else {
-                                crow[col] += val;
-                            }
+                                                ea + eb[j] + shift);
+                            old[j] = first ? ((p.beta == 0.0) ? val : fma(p.beta, old[j], val))
+                                           : old[j] + val;
                         }
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            if (j < ncol) crow[j] = old[j];
                     }
                     first = false;
                     tc_fence_before();
