@@ -7,12 +7,16 @@
 Workload "ctmrg" (default): double-layer CTMRG of the spin-1/2 Heisenberg
 model on the square lattice.  The site tensors come from the finite-temperature
 simple update (2-site checkerboard cell, tau = 0.01, second-order Trotter,
-bond dimension target D, U(1) symmetry) evolved to beta = 2 on the device; then
-SequentialCTMRG on the AB/BA cell at corner dimension chi.  One step = one CTMRG
-iteration (up, right, down, left moves).  The timed iterations start from an
-environment warmed up for W iterations; the same K iterations run once with
-the plain FP64 grouped GEMM and once with the tcgen05 Ozaki GEMM from copies of
-that environment, and the energy per bond of both runs is compared.
+bond dimension target D) evolved to beta = 2 on the device; then
+SequentialCTMRG on the AB/BA cell at corner dimension chi.  Default: SU(2)
+symmetry, D = 24 (whole multiplets: Dmax = 28), chi = 256.  `--symmetry u1`
+runs the same chain with U(1) sectors (defaults D = 12, chi = 64).  One step =
+one CTMRG iteration (up, right, down, left moves).  The timed iterations start
+from an environment warmed up for W iterations; the headline arithmetic
+(`--precision`, default ozaki7: sector GEMMs on the tcgen05 int8 tensor cores
+with 7 digit slices) runs exactly K iterations, the plain FP64 run (DMMA
+tensor cores) min(K, 3) iterations from a copy of the same environment, and the
+energies per bond after the same number of iterations are compared.
 
 Workload "u1_microbench": the U(1) kernel microbenchmark -- rank-4 float64
 tensors whose legs carry charges -4..4 with degeneracies ~ exp(-q^2/8) rounded
@@ -40,6 +44,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+METRIC = "CTMRG iter/s, grouped mixed-prec vs plain FP64 on 1 B200 at 1e-9 energy err"
 LEG_STATES = 256
 QMAX = 4
 SEED = 2024
@@ -347,23 +352,42 @@ def run_ctmrg(args, world, rank, local):
 
     from frostspin_b200 import linalg
 
-    mixed = args.precision if args.precision != "fp64" else "ozaki6"
+    mixed = args.precision if args.precision != "fp64" else "ozaki7"
     su, tensors, ctm, t_su = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
     for _ in range(args.warmup):
         ctm.iterate()
     torch.cuda.synchronize()
     start_env = ctm.copy()
+    headline_mixed = args.precision != "fp64"
+    # the headline run times exactly `steps` iterations; the comparison run
+    # (the other arithmetic, same start environment) is capped at 3 iterations
+    # and both energies are taken after the same number of iterations
+    n_cmp = min(args.steps, 3)
+    n64 = args.steps if not headline_mixed else n_cmp
+    nmx = args.steps if headline_mixed else n_cmp
     barrier(world)
-    t64, clk64, k64, l64 = timed_iterations(ctm, args.steps, "fp64", local)
-    e64 = energy_per_bond(ctm)
+    t64, clk64, k64, l64 = timed_iterations(ctm, n64, "fp64", local)
     ctm_mixed = start_env.copy()
     barrier(world)
-    tmx, clkmx, kmx, lmx = timed_iterations(ctm_mixed, args.steps, mixed, local)
-    emx = energy_per_bond(ctm_mixed)
+    tmx, clkmx, kmx, lmx = timed_iterations(ctm_mixed, nmx, mixed, local)
+    # energies after the same number of iterations from the same start
+    ref_env = ctm if n64 == n_cmp else None
+    mix_env = ctm_mixed if nmx == n_cmp else None
+    if ref_env is None:
+        ref_env = start_env.copy()
+        linalg.set_gemm_precision("fp64")
+        for _ in range(n_cmp):
+            ref_env.iterate()
+    if mix_env is None:
+        mix_env = start_env.copy()
+        linalg.set_gemm_precision(mixed)
+        for _ in range(n_cmp):
+            mix_env.iterate()
+    e64 = energy_per_bond(ref_env)
+    emx = energy_per_bond(mix_env)
     t64 = max_over_ranks(t64, world)
     tmx = max_over_ranks(tmx, world)
-    headline_mixed = args.precision != "fp64"
     t_head = tmx if headline_mixed else t64
     kern = kmx if headline_mixed else k64
 
@@ -411,8 +435,10 @@ def run_ctmrg(args, world, rank, local):
                 "launches": gem["launches"], "ms": gem["ms"]}
     perm_gbs = perm["bytes"] / (perm["ms"] * 1e-3) / 1e9
     value = world * args.steps / t_head
+    fp64_rate = world * n64 / t64
+    mixed_rate = world * nmx / tmx
     line = {
-        "metric": "CTMRG iter/s, grouped mixed-precision vs plain FP64 on 1 B200",
+        "metric": METRIC,
         "value": value,
         "unit": "iter/s",
         "n_gpus": world,
@@ -432,9 +458,10 @@ def run_ctmrg(args, world, rank, local):
             "beta": args.beta, "D_target": args.D, "Dmax": su.Dmax, "chi": args.chi,
             "chi_values": [int(c) for c in ctm.chi_values],
             "precision": mixed if headline_mixed else "fp64",
-            "fp64_iter_per_s": world * args.steps / t64,
-            "mixed_iter_per_s": world * args.steps / tmx,
-            "mixed_over_fp64": t64 / tmx,
+            "fp64_iter_per_s": fp64_rate, "fp64_steps": n64,
+            "mixed_iter_per_s": mixed_rate, "mixed_steps": nmx,
+            "mixed_over_fp64": mixed_rate / fp64_rate,
+            "energy_iterations_compared": n_cmp,
             "energy_fp64": e64, "energy_mixed": emx,
             "energy_rel_err_mixed_vs_fp64": abs(emx - e64) / abs(e64),
             "kernels_fp64_run": {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in k64.items()},
@@ -452,12 +479,71 @@ def run_ctmrg(args, world, rank, local):
         "gpu_launches": lmx if headline_mixed else l64,
         "clocks": clkmx if headline_mixed else clk64,
     }
-    if rank == 0 and not args.no_cpu_baseline and args.symmetry == "u1":
-        t_cpu, info = cpu_ctmrg_seconds(tensors, ctm_mixed, args.chi)
-        info["value"] = 1.0 / t_cpu
-        info["unit"] = "iter/s"
+    if rank == 0 and not args.no_cpu_baseline:
+        if args.symmetry == "u1":
+            t_cpu, info = cpu_ctmrg_seconds(tensors, ctm_mixed, args.chi)
+            info["value"] = 1.0 / t_cpu
+            info["unit"] = "iter/s"
+        else:
+            info = cpu_ctmrg_sample(args.symmetry, args.chi, steps=1, warmup=1)
         line["cpu_baseline"] = info
     return line
+
+
+SU_FIXTURES = {"su2": "su2_d24_beta2", "u1": "heisenberg_d12_beta2"}
+
+
+def fixture_site_tensors(symmetry):
+    """The reference's own simple-update site tensors at beta = 2 (committed
+    fixtures written by tests/golden/make_golden.py) as oracle tensors."""
+    from oracle import frostspin_oracle as fo
+    from oracle import su2_oracle as so
+
+    m = so if symmetry == "su2" else fo
+    d = np.load(os.path.join(ROOT, "tests", "golden", SU_FIXTURES[symmetry] + ".npz"))
+    out = []
+    for p in ("A0", "A1"):
+        nrr = int(d[p + "_n_row_reps"])
+        ncr = int(d[p + "_n_col_reps"])
+        irr = d[p + "_block_irreps"]
+        out.append(m.OTensor([d[f"{p}_row_rep_{i}"] for i in range(nrr)],
+                             [d[f"{p}_col_rep_{i}"] for i in range(ncr)],
+                             [d[f"{p}_block_{i}"] for i in range(irr.size)], irr,
+                             d[p + "_signature"]))
+    return out
+
+
+def cpu_ctmrg_sample(symmetry, chi_target, *, steps, warmup, chis=(8, 16)):
+    """Bounded CPU sample of the CTMRG workload: the numpy oracle (restating the
+    reference, BLAS on all host threads) from the reference's own site tensors,
+    `warmup` untimed then `steps` timed iterations at chis[0], one untimed and
+    one timed iteration at chis[1]; t(chi) = t(chis[1]) (chi / chis[1])^p with p
+    fitted on the two measured points, extrapolated to chi_target."""
+    from oracle import ctmrg_oracle as co
+
+    A, B = fixture_site_tensors(symmetry)
+    times = []
+    for chi, n_warm, n_steps in ((chis[0], warmup, steps), (chis[1], 1, 1)):
+        c = co.SequentialCTMRG(A, B, chi, cutoff=1e-10, degen_ratio=0.9999)
+        for _ in range(n_warm):
+            c.iterate()
+        t0 = time.perf_counter()
+        for _ in range(n_steps):
+            c.iterate()
+        times.append((time.perf_counter() - t0) / n_steps)
+    p = float(np.log(times[1] / times[0]) / np.log(chis[1] / chis[0]))
+    t_target = times[1] * (chi_target / chis[1]) ** max(p, 0.0)
+    return {
+        "value": 1.0 / t_target, "unit": "iter/s", "cores": os.cpu_count() or 1,
+        "kind": "port",
+        "sample": (f"numpy oracle SequentialCTMRG ({symmetry}) from the reference's own "
+                   f"simple-update tensors (D=24 target, beta=2): {times[0]:.2f} s/iteration "
+                   f"at chi={chis[0]} (mean of {steps}), {times[1]:.2f} s at chi={chis[1]}; "
+                   f"value = power-law fit (exponent {p:.2f}) extrapolated to chi={chi_target} "
+                   f"({t_target:.0f} s/iteration), labelled as an extrapolation"),
+        "measured_s_per_iter": {str(chis[0]): times[0], str(chis[1]): times[1]},
+        "fit_exponent": p, "extrapolated": True,
+    }
 
 
 def env_to_oracle(dev_ctm, chi):
@@ -692,9 +778,33 @@ def run_ours(args, world, rank, local):
     return line
 
 
+def run_reference_ctmrg(args, world):
+    """The reference arm of the CTMRG workload: the CPU oracle port (the
+    reference is Python + numba and does not travel to the GPU box)."""
+    info = cpu_ctmrg_sample(args.symmetry, args.chi, steps=args.steps, warmup=args.warmup)
+    value = info["value"]
+    return {
+        "metric": METRIC,
+        "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference's own simple-update site tensors, committed fixture)",
+        "impl": "reference",
+        "config": {"workload": f"ctmrg_heisenberg_{args.symmetry}", "beta": args.beta,
+                   "D_target": args.D, "chi": args.chi,
+                   "precision": "fp64 (numpy / OpenBLAS)",
+                   "parallelism": "host threads"},
+        "cpu_baseline": info,
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "ctmrg":
+        return run_reference_ctmrg(args, world)
     wl_states = LEG_STATES
     from frostspin_b200.symmetric_tensor.abelian_plan import GroupInfo  # noqa: F401
 
@@ -746,14 +856,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["ctmrg", "u1_microbench"], default="ctmrg")
-    ap.add_argument("--symmetry", choices=["u1", "su2"], default="u1")
+    ap.add_argument("--symmetry", choices=["u1", "su2"], default="su2")
     ap.add_argument("--D", type=int, default=None,
                     help="simple-update bond dimension target (default 12 for U(1), 24 for SU(2))")
     ap.add_argument("--chi", type=int, default=None,
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="ozaki6",
+    ap.add_argument("--precision", default="ozaki7",
                     help="sector GEMM arithmetic: fp64 or ozakiS (S = 3..8 int8 slices)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
                     help="states per leg (256 = the benchmark; smaller for profiling)")

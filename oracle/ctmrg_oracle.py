@@ -2,8 +2,9 @@
 TEST INFRASTRUCTURE ONLY.
 
 A numpy restatement of frostspin/ctmrg (ctm_contract.py, ctm_renormalize.py,
-ctm_environment.py, sequential_ctmrg.py, rdm.py) on the abelian oracle tensors
-of frostspin_oracle.py, every sector SVD on the dense path
+ctm_environment.py, sequential_ctmrg.py, rdm.py) on the oracle tensors of
+frostspin_oracle.py (U(1)/Z2) or su2_oracle.py (SU(2)), every sector SVD on the
+dense path
 (robust_svd, misc_tools/svd_tools.py:116-151).  Only tests/ and bench.py's
 CPU-baseline leg use it, as the checker and the timed CPU baseline.
 """
@@ -11,39 +12,46 @@ CPU-baseline leg use it, as the checker and the timed CPU baseline.
 import numpy as np
 
 from . import frostspin_oracle as fo
+from . import su2_oracle as so
+
+
+def module_of(o):
+    """The oracle module implementing the symmetry of an oracle tensor."""
+    return so if isinstance(o, so.OTensor) else fo
 
 
 class OT:
     """Method wrapper so the contraction recipes read like the reference."""
 
-    __slots__ = ("o",)
+    __slots__ = ("o", "m")
 
-    def __init__(self, o):
+    def __init__(self, o, m=None):
         self.o = o
+        self.m = module_of(o) if m is None else m
 
     def permute(self, r, c):
-        return OT(fo.permute(self.o, r, c))
+        return OT(self.m.permute(self.o, r, c), self.m)
 
     def __matmul__(self, other):
-        return OT(fo.matmul(self.o, other.o))
+        return OT(self.m.matmul(self.o, other.o), self.m)
 
     def transpose(self):
-        return OT(fo.transpose(self.o))
+        return OT(self.m.transpose(self.o), self.m)
 
     def dagger(self):
-        return OT(fo.dagger(self.o))
+        return OT(self.m.dagger(self.o), self.m)
 
     def norm(self):
-        return fo.norm(self.o)
+        return self.m.norm(self.o)
 
     def normalized(self):
-        return OT(fo.scale(self.o, 1.0 / fo.norm(self.o)))
+        return OT(self.m.scale(self.o, 1.0 / self.m.norm(self.o)), self.m)
 
     def full_contract(self, other):
-        return fo.full_contract(self.o, other.o)
+        return self.m.full_contract(self.o, other.o)
 
     def trace(self):
-        return fo.trace(self.o)
+        return self.m.trace(self.o)
 
     @property
     def shape(self):
@@ -88,6 +96,7 @@ def corner_dl(T4, A, C4, T3):
 
 def projectors(c1, c2, c3, c4, chi, rtol, degen_ratio):
     """Dense-SVD construct_projectors (ctm_renormalize.py:6-136)."""
+    m = c1.m
     o1, o2, o3, o4 = c1.o, c2.o, c3.o, c4.o
     shared = np.intersect1d(np.intersect1d(o1.block_irreps, o2.block_irreps),
                             np.intersect1d(o3.block_irreps, o4.block_irreps))
@@ -102,7 +111,8 @@ def projectors(c1, c2, c3, c4, chi, rtol, degen_ratio):
         us.append(u)
         ss.append(s)
         vs.append(v)
-    cuts = fo.find_block_cuts(ss, chi, rtol=rtol, degen_ratio=degen_ratio)
+    cuts = fo.find_block_cuts(ss, chi, dims=m.irrep_dims(shared), rtol=rtol,
+                              degen_ratio=degen_ratio)
     keep = np.flatnonzero(cuts)
     p_blocks, pt_blocks = [], []
     for k in keep:
@@ -111,14 +121,14 @@ def projectors(c1, c2, c3, c4, chi, rtol, degen_ratio):
         p_blocks.append(s12[:, None] * us[k][:, :c].T @ rs[k])
         pt_blocks.append(rts[k] @ vs[k][:c].T * s12)
     irr = o2.block_irreps[idx[1][keep]]
-    mid = fo.init_representation(cuts[keep], irr)
+    mid = m.init_representation(cuts[keep], irr)
     n2 = o2.nrr
     sp = np.zeros(n2 + 1, dtype=bool)
     sp[1:] = o2.signature[n2:]
     spt = np.ones(n2 + 1, dtype=bool)
     spt[:-1] = ~o2.signature[n2:]
-    P = OT(fo.transpose(fo.OTensor((mid,), o2.col_reps, p_blocks, irr, sp)))
-    Pt = OT(fo.OTensor(o2.col_reps, (mid,), pt_blocks, irr, spt))
+    P = OT(m.transpose(m.OTensor((mid,), o2.col_reps, p_blocks, irr, sp)), m)
+    Pt = OT(m.OTensor(o2.col_reps, (mid,), pt_blocks, irr, spt), m)
     return P, Pt
 
 
@@ -141,14 +151,15 @@ def ren_corner(C, T, X):
 
 def dummy_env(A):
     """ctm_environment.py:6-34 on oracle tensors."""
-    z = np.zeros(1, dtype=np.int8)
+    m = A.m
+    z = m.singlet()
     one = (z,)
     s = A.o.signature
     r = A.o.col_reps
     sh = A.o.shape
 
     def fa(arr, rr, cr, sig=None):
-        return OT(fo.from_array(arr, rr, cr, sig))
+        return OT(m.from_array(arr, rr, cr, sig), m)
 
     return {
         "C1": fa(np.eye(1), one, one),
@@ -320,7 +331,7 @@ def rdm_1x2(C1, T1l, T1r, C2, T4, Al, Ar, T2, C4, T3l, T3r, C3):
     right = right @ T3r.permute((0, 1, 2), (3,))
     right = right.permute((2, 3, 4, 5), (0, 1))
     r = (left @ right).permute((1, 3), (0, 2))
-    return fo.toarray(r.o) / r.trace()
+    return r.m.toarray(r.o) / r.trace()
 
 
 def ctm_rdm1x2(ctm, x, y):

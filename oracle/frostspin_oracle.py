@@ -298,6 +298,16 @@ def find_block_cuts(block_values, cut_target, *, dims=None, atol=0.0, rtol=None,
     return cuts
 
 
+def singlet():
+    """abelian_symmetric_tensor.py:48-50."""
+    return np.zeros(1, dtype=np.int8)
+
+
+def irrep_dims(irreps):
+    """Abelian irreps are one-dimensional."""
+    return np.ones(len(irreps), dtype=np.int64)
+
+
 def init_representation(degen, irreps):
     """abelian_symmetric_tensor.py:254-261."""
     return np.repeat(np.asarray(irreps, dtype=np.int8), np.asarray(degen, dtype=np.int64))

@@ -386,6 +386,27 @@ def case_simple_update_su2():
     save("simple_update_su2", data)
 
 
+def case_su2_d24_beta2():
+    """Site tensors of the SU(2) CTMRG benchmark: the reference's SU(2) simple
+    update of the Heisenberg model, D=24, tau=0.01, evolved to beta=2."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.simple_update import SimpleUpdate
+
+    r = np.array([[1], [2]])
+    h = SU2SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), (r, r), (r, r))
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 24, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    su.evolve(2.0)
+    data = {"beta": np.array(su.beta), "logZ": np.array(su.logZ), "Dmax": np.array(su.Dmax)}
+    for i, w in enumerate(su.get_weights()):
+        data[f"w{i}"] = w
+    for i, rep in enumerate(su.get_bond_representations()):
+        data[f"rep{i}"] = rep
+    for i, t in enumerate(su.get_tensors()):
+        pack_tensor(f"A{i}", t, data)
+    save("su2_d24_beta2", data)
+
+
 def case_heisenberg_d12_beta2():
     """Site tensors of the CTMRG benchmark: the reference's U(1) simple update of
     the Heisenberg model, D=12, tau=0.01, evolved to beta=2 (get_tensors)."""
