@@ -513,7 +513,7 @@ def fixture_site_tensors(symmetry):
     return out
 
 
-def cpu_ctmrg_sample(symmetry, chi_target, *, steps, warmup, chis=(8, 16)):
+def cpu_ctmrg_sample(symmetry, chi_target, *, steps, warmup, chis=(16, 32)):
     """Bounded CPU sample of the CTMRG workload: the numpy oracle (restating the
     reference, BLAS on all host threads) from the reference's own site tensors,
     `warmup` untimed then `steps` timed iterations at chis[0], one untimed and

@@ -407,6 +407,36 @@ def case_su2_d24_beta2():
     save("su2_d24_beta2", data)
 
 
+def _load_ref_tensor(cls, d, prefix):
+    return cls.load_from_dic(d, prefix=prefix)
+
+
+def case_corr_length():
+    """Transfer spectra and correlation lengths (abstract_ctmrg.py:519-579,
+    observables.py:4-154) after 3 CTMRG iterations at chi=20, on the SU(2)
+    simple-update tensors of simple_update_su2.npz and on the random U(1)
+    tensors of ctmrg_u1_random.npz."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.ctmrg import SequentialCTMRG
+
+    data = {}
+    for tag, cls, fix, names in (("su2", SU2SymmetricTensor, "simple_update_su2", ("A0", "A1")),
+                                 ("u1", U1SymmetricTensor, "ctmrg_u1_random", ("A", "B"))):
+        d = np.load(os.path.join(HERE, fix + ".npz"))
+        tensors = [_load_ref_tensor(cls, d, n) for n in names]
+        ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                      degen_ratio=0.9999)
+        for _ in range(3):
+            ctm.iterate()
+        for k in range(2):
+            data[f"{tag}_spec_h{k}"] = ctm.compute_transfer_spectrum_h(k, 4)
+            data[f"{tag}_spec_v{k}"] = ctm.compute_transfer_spectrum_v(k, 4)
+            data[f"{tag}_xi_h{k}"] = np.array(ctm.compute_corr_length_h(k))
+            data[f"{tag}_xi_v{k}"] = np.array(ctm.compute_corr_length_v(k))
+        data[f"{tag}_chi"] = np.array(ctm.chi_values)
+    save("corr_length", data)
+
+
 def case_heisenberg_d12_beta2():
     """Site tensors of the CTMRG benchmark: the reference's U(1) simple update of
     the Heisenberg model, D=12, tau=0.01, evolved to beta=2 (get_tensors)."""
