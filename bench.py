@@ -2,7 +2,7 @@
 """Benchmark driver: prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ctmrg|u1_microbench] [--precision fp64|ozakiS]
+                    [--workload ctmrg|u1_microbench|gemm] [--precision fp64|ozakiS]
 
 Workload "ctmrg" (default): double-layer CTMRG of the spin-1/2 Heisenberg
 model on the square lattice.  The site tensors come from the finite-temperature
@@ -25,6 +25,9 @@ with seeded N(0,1) entries (17 blocks, 455 018 564 coefficients, 3.64 GB per
 tensor).  One step = permute (0,2),(1,3) then the grouped matmul against a
 second tensor of the same structure, the hot path of every CTMRG contraction.
 Inputs are larger than the 126 MB L2, so no flush is needed between steps.
+
+Workload "gemm": one square FP64 GEMM (--gemm-n) through the grouped path at
+--precision, timed beside cuBLAS DGEMM (kernel-level measurement).
 
 Multi-GPU: the path does not shard -- every rank runs an independent replica
 (weak scaling), and the timed region is the max over ranks.
@@ -778,6 +781,56 @@ def run_ours(args, world, rank, local):
     return line
 
 
+def run_gemm(args, world, rank, local):
+    """One square FP64 GEMM (n = --gemm-n) through the grouped sector-GEMM path
+    at --precision (fp64: DMMA; ozakiS: tcgen05 int8, every problem on the int8
+    path), timed with CUDA events beside cuBLAS DGEMM on the same operands."""
+    import torch
+
+    from frostspin_b200 import linalg
+
+    n = args.gemm_n
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    C = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    spec = [{"A": A.reshape(-1), "a_off": 0, "a_trans": False, "B": B.reshape(-1), "b_off": 0,
+             "b_trans": False, "C": C.reshape(-1), "c_off": 0, "M": n, "N": n, "K": n}]
+
+    def step():
+        with linalg.gemm_precision_mode(args.precision), linalg.ozaki_dispatch_mode("all"):
+            linalg.grouped_gemm(spec)
+
+    def timed(f):
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(args.steps):
+            f()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) * 1e-3 / args.steps
+
+    t = max_over_ranks(timed(step), world)
+    linalg.check_ozaki_flags()
+    err = float((C - A @ B).abs().max() / (A.abs().max() * B.abs().max() * n))
+    t_cublas = timed(lambda: torch.matmul(A, B, out=C))
+    flops = 2.0 * n**3
+    return {
+        "metric": "square GEMM, effective FP64 TFLOP/s", "value": world * flops / t / 1e12,
+        "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else f"f64 via int8 {args.precision}",
+        "data": "synthetic (seeded N(0,1))", "impl": "ours",
+        "config": {"workload": "gemm", "n": n, "precision": args.precision,
+                   "cublas_dgemm_tflops": flops / t_cublas / 1e12,
+                   "max_err_rel_to_maxA_maxB_n": err},
+    }
+
+
 def run_reference_ctmrg(args, world):
     """The reference arm of the CTMRG workload: the CPU oracle port (the
     reference is Python + numba and does not travel to the GPU box)."""
@@ -805,6 +858,28 @@ def run_reference(args, world, rank):
         return None
     if args.workload == "ctmrg":
         return run_reference_ctmrg(args, world)
+    if args.workload == "gemm":
+        rng = np.random.default_rng(SEED)
+        n = args.gemm_n
+        A = rng.standard_normal((n, n))
+        B = rng.standard_normal((n, n))
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            A @ B
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        value = 2.0 * n**3 / float(np.mean(times)) / 1e12
+        info = {"value": value, "unit": "TFLOP/s", "cores": os.cpu_count() or 1,
+                "kind": "port", "sample": f"numpy (OpenBLAS) dgemm {n}^3, all host threads"}
+        return {"metric": "square GEMM, effective FP64 TFLOP/s", "value": value,
+                "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded N(0,1))", "impl": "reference",
+                "config": {"workload": "gemm", "n": n}, "cpu_baseline": info,
+                "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     wl_states = LEG_STATES
     from frostspin_b200.symmetric_tensor.abelian_plan import GroupInfo  # noqa: F401
 
@@ -855,7 +930,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ctmrg", "u1_microbench"], default="ctmrg")
+    ap.add_argument("--workload", choices=["ctmrg", "u1_microbench", "gemm"], default="ctmrg")
+    ap.add_argument("--gemm-n", type=int, default=4096, help="matrix size of the gemm workload")
     ap.add_argument("--symmetry", choices=["u1", "su2"], default="su2")
     ap.add_argument("--D", type=int, default=None,
                     help="simple-update bond dimension target (default 12 for U(1), 24 for SU(2))")
@@ -884,6 +960,8 @@ def main():
     world, rank, local = dist_init(args.gpus)
     if args.workload == "ctmrg":
         line = run_ctmrg(args, world, rank, local)
+    elif args.workload == "gemm":
+        line = run_gemm(args, world, rank, local)
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0:

@@ -9,7 +9,7 @@ renormalises the corner-edge-corner triple of the absorbed side.
 
 import numpy as np
 
-from . import rdm
+from . import observables, rdm
 from .ctm_contract import (
     contract_C1234,
     contract_dl,
@@ -321,6 +321,37 @@ class SequentialCTMRG:
             e.get_A(x + 1, y + 2), e.get_T2(x + 2, y + 2), e.get_C4(x, y + 3),
             e.get_T3(x + 1, y + 3), e.get_C3(x + 2, y + 3),
         )
+
+    def compute_transfer_spectrum_h(self, y, nvals, *, dmax_full=200, maxiter=1000,
+                                    arpack_tol=0):
+        """abstract_ctmrg.py:519-538: nvals largest eigenvalues of the horizontal
+        transfer matrix at cell row y."""
+        e = self._env
+        T1s = [e.get_T1(-x, y) for x in range(self.Lx)]
+        T3s = [e.get_T3(-x, y + 1) for x in range(self.Lx)]
+        return observables.compute_mps_transfer_spectrum(
+            T1s, T3s, nvals, dmax_full=dmax_full, maxiter=maxiter, arpack_tol=arpack_tol,
+            verbosity=self.verbosity)
+
+    def compute_transfer_spectrum_v(self, x, nvals, *, dmax_full=200, maxiter=1000,
+                                    arpack_tol=0):
+        """abstract_ctmrg.py:540-559 (vertical transfer matrix at cell column x)."""
+        e = self._env
+        T1s = [e.get_T2(x + 1, -y).permute((1,), (2, 3, 0)) for y in range(self.Ly)]
+        T3s = [e.get_T4(x, -y).permute((1, 2), (3, 0)) for y in range(self.Ly)]
+        return observables.compute_mps_transfer_spectrum(
+            T1s, T3s, nvals, dmax_full=dmax_full, maxiter=maxiter, arpack_tol=arpack_tol,
+            verbosity=self.verbosity)
+
+    def compute_corr_length_h(self, y, *, maxiter=1000, arpack_tol=0):
+        """abstract_ctmrg.py:561-568: -Lx / ln |lambda_2 / lambda_1|."""
+        _, v2 = self.compute_transfer_spectrum_h(y, 2, maxiter=maxiter, arpack_tol=arpack_tol)
+        return -self.Lx / np.log(np.abs(v2))
+
+    def compute_corr_length_v(self, x, *, maxiter=1000, arpack_tol=0):
+        """abstract_ctmrg.py:570-577."""
+        _, v2 = self.compute_transfer_spectrum_v(x, 2, maxiter=maxiter, arpack_tol=arpack_tol)
+        return -self.Ly / np.log(np.abs(v2))
 
     def compute_rdm_1st_neighbor_cell(self):
         r12 = [self.compute_rdm1x2(x, y) for x, y in self.site_coords]

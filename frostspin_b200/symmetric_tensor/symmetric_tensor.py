@@ -779,6 +779,86 @@ class SymmetricTensor:
             return s, u
         return s
 
+    @classmethod
+    def eigs(cls, matmat, nvals, reps, signature, *, atol=0.0, rtol=None, degen_ratio=1.0,
+             dmax_full=100, compute_vectors=False, rng=None, maxiter=4000, arpack_tol=0):
+        """symmetric_tensor.py:880-955 -> _sparse_eig (:1250-1434) for a real
+        square matrix known only through ``matmat`` (applied to device tensors).
+
+        Blocks smaller than max(dmax_full, 3k) are built by one ``matmat`` on
+        identity blocks and diagonalised on the device (torch.linalg.eigvals);
+        larger ones go to ARPACK (scipy.sparse.linalg.eigs), whose matvec copies
+        the Krylov vector to the device, applies ``matmat`` there and copies the
+        block back.  Returns the kept eigenvalues as the reference's
+        ``DiagonalTensor.toarray()`` lays them out (per kept block, each value
+        repeated irrep-dimension times), a host numpy array."""
+        if compute_vectors:
+            raise NotImplementedError("eigenvectors of a matrix-free operator are not returned")
+        import scipy.sparse.linalg as slg
+
+        if rng is None:
+            rng = np.random.default_rng()
+        m = cls.init_square_matrix(reps, signature)
+        block_irreps, block_shapes = cls.get_block_sizes(m._row_reps, m._col_reps,
+                                                         m._signature)
+        nb = len(block_shapes)
+        sigv = np.hstack((m._signature[: m._nrr], [True]))
+        dims = np.array([cls.irrep_dimension(q) for q in block_irreps], dtype=np.int64)
+        val_blocks = [None] * nb
+        abs_blocks = [np.zeros((1,))] * nb
+        full, sparse = [], []
+        for bi in range(nb):
+            k = nvals // dims[bi] + 1
+            (full if block_shapes[bi, 0] < max(dmax_full, 3 * k) else sparse).append(bi)
+
+        def keep(bi, vals, k):
+            a = np.abs(vals)
+            so = a.argsort()[: -k - 1 : -1]
+            val_blocks[bi] = vals[so]
+            abs_blocks[bi] = a[so]
+
+        if full:
+            irr_full = np.ascontiguousarray(block_irreps[full])
+            rfull = cls.init_representation(block_shapes[full, 0], irr_full)
+            eye = [torch.eye(int(block_shapes[bi, 0]), dtype=torch.float64,
+                             device=dev.device()) for bi in full]
+            st = matmat(cls(m._row_reps, (rfull,), eye, irr_full, sigv))
+            for bi in full:
+                q = block_irreps[bi]
+                bj = int(np.searchsorted(st.block_irreps, q))
+                if bj < st.nblocks and st.block_irreps[bj] == q:
+                    vals = torch.linalg.eigvals(st.blocks[bj]).cpu().numpy()
+                    keep(bi, vals, nvals // dims[bi] + 1)
+        for bi in sparse:
+            q = block_irreps[bi : bi + 1]
+            d = int(block_shapes[bi, 0])
+            k = nvals // dims[bi] + 1
+            v0 = rng.standard_normal(size=(d,))
+            brep = cls.init_representation(np.ones((1,), dtype=np.int64), q)
+            st0 = cls(m._row_reps, (brep,), (v0[:, None],), q, sigv)
+            st1 = matmat(st0)
+            bj = int(np.searchsorted(st1.block_irreps, q[0]))
+            if not (bj < st1.nblocks and st1.block_irreps[bj] == q[0]):
+                continue
+
+            def matvec(x, st0=st0, bj=bj):
+                st0.blocks[0][:, 0].copy_(torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)))
+                return matmat(st0).blocks[bj].reshape(-1).cpu().numpy()
+
+            op = slg.LinearOperator((d, d), matvec=matvec, dtype=np.float64)
+            try:
+                vals = slg.eigs(op, k=k, v0=v0, maxiter=maxiter, tol=arpack_tol,
+                                return_eigenvectors=False)
+            except slg.ArpackNoConvergence as err:
+                vals = err.eigenvalues
+            keep(bi, vals, k)
+        cuts = find_block_cuts(abs_blocks, nvals, dims=dims, atol=atol, rtol=rtol,
+                               degen_ratio=degen_ratio)
+        kept = [bi for bi in range(nb) if cuts[bi]]
+        dtype = np.result_type(*[val_blocks[bi].dtype for bi in kept]) if kept else np.float64
+        out = [np.repeat(val_blocks[bi][: cuts[bi]].astype(dtype), dims[bi]) for bi in kept]
+        return np.concatenate(out) if out else np.zeros(0, dtype=dtype)
+
     @staticmethod
     def _irrep_key(q):
         return int(q) if np.ndim(q) == 0 else tuple(np.ravel(q))

@@ -35,3 +35,38 @@ def test_sequential_ctmrg_matches_reference():
         assert ctm.chi_values == list(d[f"it{it}_chi"])
         logz = ctm.compute_PEPS_norm_log()
         assert abs(logz - float(d[f"it{it}_logZ"])) < tol * 10
+
+
+@pytest.mark.parametrize("tag", ["su2", "u1"])
+def test_transfer_spectrum_and_corr_length_match_reference(tag):
+    """abstract_ctmrg.py:519-579 / observables.py:4-154 on the device against the
+    reference's values after 3 CTMRG iterations at chi=20: the 4 leading
+    transfer eigenvalues (as a multiset; conjugate pairs may come in either
+    order) and the correlation lengths, horizontal and vertical."""
+    from frostspin_b200 import SU2SymmetricTensor, U1SymmetricTensor
+    from frostspin_b200.ctmrg import SequentialCTMRG
+
+    ref = load("corr_length")
+    if tag == "su2":
+        d = load("simple_update_su2")
+        tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
+    else:
+        d = load("ctmrg_u1_random")
+        tensors = [U1SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A", "B")]
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for _ in range(3):
+        ctm.iterate()
+    assert np.array_equal(ctm.chi_values, ref[f"{tag}_chi"])
+    for k in range(2):
+        for kind, fn in (("h", ctm.compute_transfer_spectrum_h),
+                         ("v", ctm.compute_transfer_spectrum_v)):
+            got = np.asarray(fn(k, 4))
+            exp = np.asarray(ref[f"{tag}_spec_{kind}{k}"])
+            key = lambda z: (round(float(np.abs(z)), 9), round(float(np.imag(z)), 9))  # noqa: E731
+            for a, b in zip(sorted(got, key=key), sorted(exp, key=key), strict=True):
+                assert abs(a - b) < 1e-8, (kind, k, got, exp)
+        xh = ctm.compute_corr_length_h(k)
+        xv = ctm.compute_corr_length_v(k)
+        assert abs(xh - float(ref[f"{tag}_xi_h{k}"])) < 1e-7 * float(ref[f"{tag}_xi_h{k}"])
+        assert abs(xv - float(ref[f"{tag}_xi_v{k}"])) < 1e-7 * float(ref[f"{tag}_xi_v{k}"])
