@@ -144,6 +144,7 @@ SIGNATURES = {
     "fs_ozaki_geometry": (ctypes.c_int, [_P, _P, _P, _P]),
     "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
+    "fs_ozaki_gemm_pair": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "fs_ozaki_gemm_noalloc": (ctypes.c_int, [_P, _I64, _I32, _P]),
     "fs_scale": (ctypes.c_int, [_P, _I64, _D, _P]),
     "fs_axpby": (ctypes.c_int, [_P, _P, _I64, _D, _D, _P]),
@@ -196,7 +197,7 @@ CALL_COUNTS = {}
 
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
-    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1,
+    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
     "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1,
 }

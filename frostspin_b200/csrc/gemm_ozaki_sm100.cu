@@ -478,6 +478,361 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ------------------------------------------------------- CTA-pair GEMM kernel
+//
+// The same arithmetic on 256 x 256 output tiles, computed by a cluster of two
+// CTAs with tcgen05.mma.cta_group::2 (M = 256, N = 256).  CTA r of the pair
+// loads its own 128 rows of the A slice tile (row tile 2 tm + r) and its own
+// 128 rows of the B^T slice tile (row tile 2 tn + r) into its own shared
+// memory: half the bytes per SM of the single-CTA kernel for the same MMA work.
+// The even CTA issues the MMAs, which read A from each CTA and B from both, and
+// accumulate rows [128 r, 128 r + 128) of the tile in CTA r's TMEM.
+//
+// Handshakes (all waits bounded):
+//   full[s]      each CTA: its own bulk copies of stage s landed (complete_tx);
+//   peer_full[s] even CTA: the odd CTA's relay thread saw its full[s] complete
+//                and arrived remotely;
+//   empty[s]     both CTAs: the MMAs reading stage s finished (the even CTA's
+//                commit arrives on both CTAs' barriers);
+//   acc_full[b]  both CTAs: accumulator b holds a finished diagonal chunk;
+//   acc_empty[b] even CTA: the 8 epilogue warps of the pair drained buffer b
+//                (4 local arrivals, 4 remote ones from the odd CTA).
+// A cluster barrier after the MMA drain keeps both CTAs (their shared memory
+// and TMEM) alive until no MMA can touch them.  No load uses multicast.
+
+constexpr int kPairStages = 6;
+constexpr int kPairStageBytes = 2 * kABytes;                // 16 KB A half + 16 KB B half
+constexpr uint32_t kIdescPair = (2u << 4) | (1u << 7) | (1u << 10) |
+                                (static_cast<uint32_t>(kTileN >> 3) << 17) |
+                                (static_cast<uint32_t>(256 >> 4) << 24);
+
+struct __align__(8) PairBarriers {
+    uint64_t full[kPairStages];
+    uint64_t peer_full[kPairStages];
+    uint64_t empty[kPairStages];
+    uint64_t acc_full[2];
+    uint64_t acc_empty[2];
+    uint64_t mma_drain;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the same shared variable in CTA `rank`
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t addr, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(addr), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
+                     cluster_addr)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdescPair), "r"(accumulate)
+        : "memory");
+}
+
+// commit of the pair's MMAs to this CTA's barrier at `bar`
+__device__ __forceinline__ void mma_commit_pair_local(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+// commit of the pair's MMAs arriving on the barrier at this shared offset in
+// both CTAs of the pair (commit multicast; no load is multicast)
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+        "[%0], %1;" ::"r"(bar),
+        "h"(mask)
+        : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    k_oz_gemm_pair(const FsOzProblem* __restrict__ probs, int64_t n_probs,
+                   const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
+                   int chunk_ktiles, int32_t* flag) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* smem = smem_raw + (base - raw);
+    PairBarriers* bars = reinterpret_cast<PairBarriers*>(smem + kPairStages * kPairStageBytes);
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t rank = cluster_ctarank();
+    const int64_t cluster_id = blockIdx.x / 2;
+    const int64_t n_clusters = gridDim.x / 2;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kPairStages; ++s) {
+            mbar_init(smem_addr(&bars->full[s]), 1);
+            mbar_init(smem_addr(&bars->peer_full[s]), 1);
+            mbar_init(smem_addr(&bars->empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_addr(&bars->acc_full[b]), 1);
+            mbar_init(smem_addr(&bars->acc_empty[b]), 8);
+        }
+        mbar_init(smem_addr(&bars->mma_drain), 1);
+        bars->abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(&bars->tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        tc_fence_before();
+    }
+    __syncthreads();
+    cluster_sync_all();  // barriers of both CTAs initialised before any remote arrive
+    tc_fence_after();
+    const uint32_t tmem_base = bars->tmem_base;
+    volatile int* abort_flag = &bars->abort_flag;
+
+    if (warp == 0) {
+        // ------------------------------------------ producer (both CTAs)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            uint32_t issued_mask = 0, issued_parity = 0;
+            for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
+                const FsOzTile tile = tiles[t];
+                const FsOzProblem p = probs[tile.problem];
+                const int64_t a_slice = static_cast<int64_t>(p.ktiles) * p.a_rowtiles * kABytes;
+                const int64_t b_slice = static_cast<int64_t>(p.ktiles) * p.b_rowtiles * kABytes;
+                const int a_rt = 2 * tile.tm + static_cast<int>(rank);
+                const int b_rt = 2 * tile.tn + static_cast<int>(rank);
+                for (int d = nslices - 1; ok && d >= 0; --d) {
+                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
+                        for (int s = 0; ok && s <= d; ++s) {
+                            for (int kt = k0; kt < k1; ++kt) {
+                                if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1,
+                                               abort_flag)) {
+                                    ok = false;
+                                    break;
+                                }
+                                const uint32_t full = smem_addr(&bars->full[stage]);
+                                mbar_expect_tx(full, kPairStageBytes);
+                                const int8_t* a = p.a_slices + s * a_slice +
+                                                  (static_cast<int64_t>(kt) * p.a_rowtiles + a_rt) * kABytes;
+                                const int8_t* b = p.b_slices + (d - s) * b_slice +
+                                                  (static_cast<int64_t>(kt) * p.b_rowtiles + b_rt) * kABytes;
+                                const uint32_t dst = base + stage * kPairStageBytes;
+                                bulk_g2s(dst, a, kABytes, full);
+                                bulk_g2s(dst + kABytes, b, kABytes, full);
+                                issued_mask |= 1u << stage;
+                                issued_parity = (issued_parity & ~(1u << stage)) | (phase << stage);
+                                if (++stage == kPairStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            for (int s = 0; s < kPairStages; ++s) {
+                if (issued_mask & (1u << s)) {
+                    if (!mbar_wait_drain(smem_addr(&bars->full[s]), (issued_parity >> s) & 1u))
+                        *abort_flag = 1;
+                }
+            }
+        }
+    } else if (warp == 1 && rank == 1) {
+        // ---------------------------- relay (odd CTA): stage s landed here
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
+                const FsOzProblem p = probs[tiles[t].problem];
+                for (int d = nslices - 1; ok && d >= 0; --d) {
+                    const int64_t n_fill = static_cast<int64_t>(d + 1) * p.ktiles;
+                    for (int64_t f = 0; f < n_fill; ++f) {
+                        if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_arrive_remote(map_to_rank(smem_addr(&bars->peer_full[stage]), 0));
+                        if (++stage == kPairStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------ MMA issuer (even CTA)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool ok = true;
+            for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
+                const FsOzProblem p = probs[tiles[t].problem];
+                for (int d = nslices - 1; ok && d >= 0; --d) {
+                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
+                        if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1,
+                                       abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t tmem_d = tmem_base + acc * kTileN;
+                        uint32_t accumulate = 0;
+                        for (int s = 0; ok && s <= d; ++s) {
+                            for (int kt = k0; kt < k1; ++kt) {
+                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag) ||
+                                    !mbar_wait(smem_addr(&bars->peer_full[stage]), phase,
+                                               abort_flag)) {
+                                    ok = false;
+                                    break;
+                                }
+                                tc_fence_after();
+                                const uint32_t a_addr = base + stage * kPairStageBytes;
+                                const uint32_t b_addr = a_addr + kABytes;
+#pragma unroll
+                                for (int k = 0; k < kTileK / 32; ++k) {
+                                    mma_i8_pair(tmem_d, smem_desc_sw128(a_addr + 32 * k),
+                                                smem_desc_sw128(b_addr + 32 * k), accumulate);
+                                    accumulate = 1;
+                                }
+                                mma_commit_pair(smem_addr(&bars->empty[stage]));
+                                if (++stage == kPairStages) {
+                                    stage = 0;
+                                    phase ^= 1;
+                                }
+                            }
+                        }
+                        if (!ok) break;
+                        mma_commit_pair(smem_addr(&bars->acc_full[acc]));
+                        if (++acc == 2) {
+                            acc = 0;
+                            acc_phase ^= 1;
+                        }
+                    }
+                }
+            }
+            mma_commit_pair_local(smem_addr(&bars->mma_drain));
+            if (!mbar_wait_drain(smem_addr(&bars->mma_drain), 0)) *abort_flag = 1;
+        }
+    } else {
+        // ------------------------------------------ epilogue (both CTAs)
+        const int quad = warp % 4;
+        const int row_in_tile = static_cast<int>(rank) * 128 + quad * 32 + lane;
+        const uint32_t acc_empty_leader[2] = {
+            map_to_rank(smem_addr(&bars->acc_empty[0]), 0),
+            map_to_rank(smem_addr(&bars->acc_empty[1]), 0)};
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        bool ok = true;
+        for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
+            const FsOzTile tile = tiles[t];
+            const FsOzProblem p = probs[tile.problem];
+            const int64_t row = static_cast<int64_t>(tile.tm) * 256 + row_in_tile;
+            const int col0 = tile.tn * kTileN;
+            const bool row_ok = row < p.M;
+            const int ea = row_ok ? p.a_exps[row] : 0;
+            bool first = true;
+            for (int d = nslices - 1; ok && d >= 0; --d) {
+                for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
+                    int got = 0;
+                    if (lane == 0)
+                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag)
+                                  ? 1
+                                  : 0;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (!got) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) +
+                                           acc * kTileN;
+                    const int shift = -7 * (d + 2);
+                    const bool read_c = !first || p.beta != 0.0;
+                    for (int cb = 0; cb < kTileN; cb += 16) {
+                        uint32_t v[16];
+                        tmem_ld16(taddr + cb, v);
+                        if (!row_ok || col0 + cb >= p.N) continue;
+                        double* crow = p.C + row * p.ldc + col0 + cb;
+                        const int32_t* be = p.b_exps + col0 + cb;
+                        const int ncol = min(16, p.N - col0 - cb);
+                        double old[16];
+                        int eb[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            eb[j] = (j < ncol) ? __ldg(be + j) : 0;
+                            old[j] = (read_c && j < ncol) ? crow[j] : 0.0;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const double val =
+                                p.alpha * ldexp(static_cast<double>(static_cast<int32_t>(v[j])),
+                                                ea + eb[j] + shift);
+                            old[j] = first ? ((p.beta == 0.0) ? val : fma(p.beta, old[j], val))
+                                           : old[j] + val;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            if (j < ncol) crow[j] = old[j];
+                    }
+                    first = false;
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (rank == 0)
+                            mbar_arrive(smem_addr(&bars->acc_empty[acc]));
+                        else
+                            mbar_arrive_remote(acc_empty_leader[acc]);
+                    }
+                    if (++acc == 2) {
+                        acc = 0;
+                        acc_phase ^= 1;
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    cluster_sync_all();  // no MMA of the pair can touch either CTA after this
+    if (threadIdx.x == 0 && *abort_flag) raise_flag(flag, FS_ERR_TIMEOUT);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
 }  // namespace oz
 }  // namespace fsb
 
@@ -536,6 +891,35 @@ extern "C" int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
     }
     const int grid = static_cast<int>(n_tiles < fsb::kNumSM ? n_tiles : fsb::kNumSM);
     fsb::oz::k_oz_gemm<<<grid, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
+        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
+    return fsb::launch_status();
+}
+
+extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
+                                  const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
+                                  int32_t chunk_ktiles, int32_t* d_flag, void* stream) {
+    if (n_probs < 0 || n_tiles < 0 || chunk_ktiles < 1) return FS_ERR_INVALID_ARG;
+    if (nslices < 1 || nslices > FS_OZAKI_MAX_SLICES) return FS_ERR_INVALID_ARG;
+    if (n_tiles == 0) return FS_OK;
+    if (d_probs == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    const long long bound = static_cast<long long>(nslices) * chunk_ktiles * fsb::oz::kTileK *
+                            127LL * 127LL;
+    if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
+    const int smem = fsb::oz::kPairStages * fsb::oz::kPairStageBytes +
+                     static_cast<int>(sizeof(fsb::oz::PairBarriers)) + 1024;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fsb::oz::k_oz_gemm_pair,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) {
+            fsb::set_last_cuda_error(e);
+            return FS_ERR_CUDA;
+        }
+        configured = true;
+    }
+    const int64_t max_clusters = fsb::kNumSM / 2;
+    const int clusters = static_cast<int>(n_tiles < max_clusters ? n_tiles : max_clusters);
+    fsb::oz::k_oz_gemm_pair<<<2 * clusters, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
         d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
     return fsb::launch_status();
 }

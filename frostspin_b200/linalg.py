@@ -16,7 +16,7 @@ from . import instrument
 
 # ----------------------------------------------------------------- precision
 
-_PRECISION = {"gemm": "fp64", "dispatch": "cost"}
+_PRECISION = {"gemm": "fp64", "dispatch": "cost", "pair": False}
 PRECISIONS = ("fp64",) + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
 
 
@@ -57,6 +57,20 @@ def ozaki_dispatch_mode(kind):
         yield
     finally:
         _PRECISION["dispatch"] = old
+
+
+@contextlib.contextmanager
+def ozaki_pair_mode(enabled):
+    """Whether Ozaki problems with more than 128 rows run on CTA pairs
+    (fs_ozaki_gemm_pair) or on single CTAs (fs_ozaki_gemm, the default: the
+    pair kernel waits for its peer's operand copies through a relay thread and
+    measures slower, 53 vs 79 TF/s effective at 8192^3 with S = 6)."""
+    old = _PRECISION["pair"]
+    _PRECISION["pair"] = bool(enabled)
+    try:
+        yield
+    finally:
+        _PRECISION["pair"] = old
 
 
 # ------------------------------------------------------------- grouped GEMM
@@ -167,10 +181,11 @@ def grouped_dgemm_table(arr, region="gemm_fp64"):
             _dgemm(sub, None, tm, tn, ntile)
 
 
-# rough rates of the two paths on B200 (measured on the U(1) microbench), used
-# only to decide which path a sector GEMM takes in a mixed-precision run
-_INT8_OPS = 1.1e15
-_FP64_FLOPS = 1.1e13
+# rates of the two paths on B200 (int8: k_oz_gemm inside the SU(2) CTMRG
+# workload; FP64: the DMMA tile kernel on large sectors), used only to decide
+# which path a sector GEMM takes in a mixed-precision run
+_INT8_OPS = 1.3e15
+_FP64_FLOPS = 2.8e13
 _EPILOGUE_BPS = 2.0e12
 _SPLIT_BPS = 3.0e12
 
@@ -193,7 +208,7 @@ def ozaki_pays(arr, S):
     K = arr["K"].astype(np.float64)
     t_oz = (S * (S + 1) / 2 * 2 * _pad(M, 128) * _pad(N, 256) * _pad(np.maximum(K, 1), 128)
             / _INT8_OPS + S * M * N * 16 / _EPILOGUE_BPS + (M * K + K * N) * (8 + S) / _SPLIT_BPS)
-    t_64 = 2 * M * N * K / _FP64_FLOPS
+    t_64 = 2 * _pad(M, 64) * _pad(N, 64) * K / _FP64_FLOPS
     return t_oz < t_64
 
 
@@ -295,20 +310,27 @@ def _round_up(x, a):
     return (x + a - 1) // a * a
 
 
-def ozaki_plan(arr, nslices):
+def ozaki_plan(arr, nslices, pair=False):
     """Operand/problem/tile tables and workspace layout for a problem array
-    (GEMM_PROBLEM_DTYPE).  Returns (ops, probs, tiles, workspace_bytes, offsets)
-    with pointer fields relative to the workspace base (patched on launch)."""
+    (GEMM_PROBLEM_DTYPE).  Returns (ops, probs, tiles, pair_tiles,
+    workspace_bytes) with pointer fields relative to the workspace base
+    (patched on launch).  With `pair`, problems of more than 128 rows get an
+    even number of A row tiles and 256-row tiles in `pair_tiles` (CTA-pair
+    kernel); the others stay in `tiles`."""
     n = arr.size
     ops = np.zeros(2 * n, dtype=_native.OZ_OPERAND_DTYPE)
     probs = np.zeros(n, dtype=_native.OZ_PROBLEM_DTYPE)
     off = 0
     rel = {"a_slices": [], "b_slices": [], "a_exps": [], "b_exps": []}
     tiles = []
+    pair_tiles = []
     for i in range(n):
         M, N, K = int(arr["M"][i]), int(arr["N"][i]), int(arr["K"][i])
         kt = max(1, (K + OZ_TILE_K - 1) // OZ_TILE_K)
         art = (M + OZ_SPLIT_ROWS - 1) // OZ_SPLIT_ROWS
+        is_pair = pair and M > OZ_TILE_M
+        if is_pair:
+            art += art % 2
         brt = 2 * ((N + OZ_TILE_N - 1) // OZ_TILE_N)
         a_bytes = nslices * kt * art * OZ_TILE_BYTES
         b_bytes = nslices * kt * brt * OZ_TILE_BYTES
@@ -325,27 +347,30 @@ def ozaki_plan(arr, nslices):
         ops[2 * i + 1] = (arr["B"][i], ldb if tb else 1, 1 if tb else ldb, b_sl, b_ex, N, K, brt, kt)
         probs[i] = (a_sl, b_sl, a_ex, b_ex, arr["C"][i], arr["ldc"][i], M, N, K, art, brt, kt,
                     arr["alpha"][i], arr["beta"][i])
-        for tm_ in range(art):
+        for tm_ in range(art // 2 if is_pair else art):
             for tn_ in range((N + OZ_TILE_N - 1) // OZ_TILE_N):
-                tiles.append((i, tm_, tn_, 0, K))
+                (pair_tiles if is_pair else tiles).append((i, tm_, tn_, 0, K))
         rel["a_slices"].append(a_sl)
-    tile_arr = np.zeros(len(tiles), dtype=_native.OZ_TILE_DTYPE)
-    if tiles:
-        t = np.array(tiles, dtype=np.int64)
-        order = np.argsort(-t[:, 4], kind="stable")
-        t = t[order]
-        tile_arr["problem"] = t[:, 0]
-        tile_arr["tm"] = t[:, 1]
-        tile_arr["tn"] = t[:, 2]
-    return ops, probs, tile_arr, off
+
+    def table(lst):
+        out = np.zeros(len(lst), dtype=_native.OZ_TILE_DTYPE)
+        if lst:
+            t = np.array(lst, dtype=np.int64)
+            t = t[np.argsort(-t[:, 4], kind="stable")]
+            out["problem"] = t[:, 0]
+            out["tm"] = t[:, 1]
+            out["tn"] = t[:, 2]
+        return out
+
+    return ops, probs, table(tiles), table(pair_tiles), off
 
 
 def ozaki_gemm(arr, nslices, workspace=None):
     """Run the problems of `arr` (GEMM_PROBLEM_DTYPE) on the tcgen05 Ozaki path.
     The workspace is a caller-owned uint8 device buffer (allocated here from
     torch's caching allocator when not given)."""
-    ops, probs, tiles, nbytes = ozaki_plan(arr, nslices)
-    if tiles.size == 0:
+    ops, probs, tiles, pair_tiles, nbytes = ozaki_plan(arr, nslices, _PRECISION["pair"])
+    if tiles.size == 0 and pair_tiles.size == 0:
         return
     if workspace is None or workspace.numel() < nbytes:
         workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev.device())
@@ -356,7 +381,6 @@ def ozaki_gemm(arr, nslices, workspace=None):
         probs[f] += np.uint64(base)
     d_ops = dev.upload(ops)
     d_probs = dev.upload(probs)
-    d_tiles = dev.upload(tiles)
     max_rows = int(ops["rows"].max())
     max_tiles = int((ops["rowtiles"].astype(np.int64) * ops["ktiles"]).max())
     for start in range(0, ops.size, 65534):
@@ -371,17 +395,21 @@ def ozaki_gemm(arr, nslices, workspace=None):
             dev.stream(),
         )
     flag = torch.zeros(1, dtype=torch.int32, device=dev.device())
-    _native.call(
-        "fs_ozaki_gemm",
-        d_probs.data_ptr(),
-        probs.size,
-        d_tiles.data_ptr(),
-        tiles.size,
-        nslices,
-        ozaki_chunk_ktiles(nslices),
-        flag.data_ptr(),
-        dev.stream(),
-    )
+    for entry, tl in (("fs_ozaki_gemm_pair", pair_tiles), ("fs_ozaki_gemm", tiles)):
+        if tl.size == 0:
+            continue
+        d_tiles = dev.upload(tl)
+        _native.call(
+            entry,
+            d_probs.data_ptr(),
+            probs.size,
+            d_tiles.data_ptr(),
+            tl.size,
+            nslices,
+            ozaki_chunk_ktiles(nslices),
+            flag.data_ptr(),
+            dev.stream(),
+        )
     _OZ_FLAGS.append(flag)
     if len(_OZ_FLAGS) > 64:
         check_ozaki_flags()

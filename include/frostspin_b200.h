@@ -211,6 +211,16 @@ int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
                   int32_t chunk_ktiles, int32_t* d_flag, void* stream);
 
 /*
+ * The same GEMM on 256 x 256 output tiles computed by clusters of two CTAs
+ * (tcgen05.mma.cta_group::2, each CTA loading half of every operand stage).
+ * Tiles index 256-row blocks of C (tm) and 256-column blocks (tn); every
+ * problem listed in d_tiles must have an even a_rowtiles.
+ */
+int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
+                       const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
+                       int32_t chunk_ktiles, int32_t* d_flag, void* stream);
+
+/*
  * Grouped Ozaki GEMM that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory: a host application whose own

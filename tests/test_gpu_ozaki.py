@@ -89,3 +89,28 @@ def test_ozaki_accuracy_vs_fp64(S):
         err = np.abs(C - R) / scale
         # dropped digits beyond S of each operand and dropped diagonals d >= S
         assert err.max() < 2.0 * S * 2.0 ** (-7 * S), (S, err.max())
+
+
+@pytest.mark.parametrize("S", [4, 7])
+def test_ozaki_pair_kernel_bit_exact(S):
+    """Problems above 128 rows run on CTA pairs (tcgen05 cta_group::2); the
+    result is bit-identical to the single-CTA kernel and to the emulation,
+    including odd row-tile counts (padded) and ragged edges."""
+    from frostspin_b200 import _native, linalg
+
+    rng = np.random.default_rng(50 + S)
+    shapes = [(129, 300, 200), (384, 256, 128), (600, 700, 300), (257, 5, 1000), (1024, 512, 640)]
+    probs = []
+    for i, (m, n, k) in enumerate(shapes):
+        A = rng.standard_normal((m, k)) * np.exp(rng.normal(0, 2, size=(m, 1)))
+        B = rng.standard_normal((k, n))
+        probs.append((A, B, bool(i % 2), bool(i % 3 == 1)))
+    before = _native.CALL_COUNTS.get("fs_ozaki_gemm_pair", 0)
+    with linalg.ozaki_pair_mode(True):
+        pair = run_grouped(probs, f"ozaki{S}")
+    assert _native.CALL_COUNTS.get("fs_ozaki_gemm_pair", 0) > before
+    with linalg.ozaki_pair_mode(False):
+        single = run_grouped(probs, f"ozaki{S}")
+    for (A, B, _, _), cp, cs in zip(probs, pair, single, strict=True):
+        assert np.array_equal(cp, cs)
+        assert np.array_equal(cp, emulate(A, B, S))
