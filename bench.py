@@ -337,10 +337,13 @@ def timed_iterations(ctm, steps, precision, local):
     clocks.start()
     s = torch.cuda.Event(enable_timing=True)
     e = torch.cuda.Event(enable_timing=True)
+    # NVTX range for profilers: "timed_fp64" or "timed_mixed"
+    torch.cuda.nvtx.range_push("timed_fp64" if precision == "fp64" else "timed_mixed")
     s.record()
     for _ in range(steps):
         ctm.iterate()
     e.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     clk = clocks.stop()
     instrument.disable()

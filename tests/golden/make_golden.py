@@ -437,6 +437,43 @@ def case_corr_length():
     save("corr_length", data)
 
 
+def case_ctmrg_su2_d24():
+    """SU(2) SequentialCTMRG from the reference's D=24 simple-update tensors
+    (su2_d24_beta2.npz) at chi=24, 2 iterations: chi values, rdms, energy."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.ctmrg import SequentialCTMRG
+
+    import tempfile
+
+    from frostspin.groups.su2_clebsch_gordan import save_su2_cg
+
+    # the reference's shipped CG table stops at irrep dimension 10; these
+    # corners need larger irreps, so the reference's own generator writes a
+    # table up to 18 first (a transient file, deleted afterwards)
+    with tempfile.TemporaryDirectory(dir=HERE) as tmp:
+        cg_file = os.path.join(tmp, "cg18.npz")
+        save_su2_cg(cg_file, 18)
+        SU2SymmetricTensor.reload_clebsch_gordan(cg_file)
+    d = np.load(os.path.join(HERE, "su2_d24_beta2.npz"))
+    tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 24, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    data = {}
+    for it in range(2):
+        ctm.iterate()
+        data[f"it{it}_chi"] = np.array(ctm.chi_values)
+    h = SDS_22.reshape(2, 2, 2, 2)
+    es = []
+    for (x, y) in ctm.site_coords:
+        r12 = ctm.compute_rdm1x2(x, y).toarray()
+        r21 = ctm.compute_rdm2x1(x, y).toarray()
+        data[f"rdm1x2_{x}{y}"] = r12
+        data[f"rdm2x1_{x}{y}"] = r21
+        es += [np.einsum("ijkl,klij->", r12, h), np.einsum("ijkl,klij->", r21, h)]
+    data["energy"] = np.array(np.mean(es))
+    save("ctmrg_su2_d24", data)
+
+
 def case_heisenberg_d12_beta2():
     """Site tensors of the CTMRG benchmark: the reference's U(1) simple update of
     the Heisenberg model, D=12, tau=0.01, evolved to beta=2 (get_tensors)."""

@@ -70,3 +70,28 @@ def test_su2_simple_update_then_ctmrg_matches_reference():
             got = fn(x, y).toarray()
             assert np.abs(got - d[f"{kind}_{x}{y}"]).max() < 1e-8
     assert abs(ctm.compute_PEPS_norm_log() - float(d["logZ_ctm"])) < 1e-8
+
+
+def test_su2_simple_update_d24_matches_reference():
+    """The benchmark's simple update (SU(2), D=24 target, tau=0.01) evolved to
+    beta=2 on the device against the reference's own run: Dmax, bond
+    representations (bit-exact truncation decisions over 200 Trotter steps),
+    weights and logZ."""
+    from frostspin_b200 import SU2SymmetricTensor
+    from frostspin_b200.simple_update import SimpleUpdate
+
+    d = load("su2_d24_beta2")
+    r = np.array([[1], [2]])
+    sds = np.array([[0.25, 0, 0, 0], [0, -0.25, 0.5, 0], [0, 0.5, -0.25, 0],
+                    [0, 0, 0, 0.25]]).reshape(2, 2, 2, 2)
+    h = SU2SymmetricTensor.from_array(sds, (r, r), (r, r))
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 24, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    su.evolve(2.0)
+    assert abs(su.beta - float(d["beta"])) < 1e-12
+    assert su.Dmax == int(d["Dmax"])
+    for i, rep in enumerate(su.get_bond_representations()):
+        assert np.array_equal(rep, d[f"rep{i}"])
+    for i, w in enumerate(su.get_weights()):
+        np.testing.assert_allclose(w, d[f"w{i}"], rtol=1e-8, atol=1e-12)
+    assert abs(su.logZ - float(d["logZ"])) < 1e-10
