@@ -464,6 +464,7 @@ def run_ctmrg(args, world, rank, local):
             "beta": args.beta, "D_target": args.D, "Dmax": su.Dmax, "chi": args.chi,
             "chi_values": [int(c) for c in ctm.chi_values],
             "precision": mixed if headline_mixed else "fp64",
+            "ozaki_pair": args.ozaki_pair,
             "fp64_iter_per_s": fp64_rate, "fp64_steps": n64,
             "mixed_iter_per_s": mixed_rate, "mixed_steps": nmx,
             "mixed_over_fp64": mixed_rate / fp64_rate,
@@ -942,6 +943,8 @@ def main():
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ozaki-pair", choices=["on", "off"], default="on",
+                    help="large int8 sector GEMMs on CTA pairs (tcgen05 cta_group::2)")
     ap.add_argument("--precision", default="ozaki7",
                     help="sector GEMM arithmetic: fp64 or ozakiS (S = 3..8 int8 slices)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
@@ -961,6 +964,9 @@ def main():
             print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_init(args.gpus)
+    from frostspin_b200 import linalg
+
+    linalg.set_ozaki_pair(args.ozaki_pair == "on")
     if args.workload == "ctmrg":
         line = run_ctmrg(args, world, rank, local)
     elif args.workload == "gemm":

@@ -20,6 +20,7 @@
 // without tensor maps.  All device waits are bounded: on timeout the kernel
 // raises FS_ERR_TIMEOUT in the caller's flag, drains its copies, frees TMEM
 // and returns.
+#include <cuda.h>
 #include <math.h>
 
 #include <algorithm>
@@ -488,17 +489,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 // The even CTA issues the MMAs, which read A from each CTA and B from both, and
 // accumulate rows [128 r, 128 r + 128) of the tile in CTA r's TMEM.
 //
-// Handshakes (all waits bounded):
-//   full[s]      each CTA: its own bulk copies of stage s landed (complete_tx);
-//   peer_full[s] even CTA: the odd CTA's relay thread saw its full[s] complete
-//                and arrived remotely;
+// Operand tiles are fetched by TMA through a 2-D tensor map that views the
+// slice workspace as rows of 128 bytes (box 128 x 128, no swizzle: the split
+// kernels already wrote the swizzled layout).  The loads carry .cta_group::2,
+// so both CTAs' copies complete on the even CTA's barrier.  Handshakes (all
+// waits bounded):
+//   full[s]      even CTA: both CTAs' 2 x 32 KB of stage s landed (the even
+//                CTA arrives once with the expected byte count);
 //   empty[s]     both CTAs: the MMAs reading stage s finished (the even CTA's
 //                commit arrives on both CTAs' barriers);
 //   acc_full[b]  both CTAs: accumulator b holds a finished diagonal chunk;
 //   acc_empty[b] even CTA: the 8 epilogue warps of the pair drained buffer b
 //                (4 local arrivals, 4 remote ones from the odd CTA).
-// A cluster barrier after the MMA drain keeps both CTAs (their shared memory
-// and TMEM) alive until no MMA can touch them.  No load uses multicast.
+// A cluster barrier after the MMA and copy drains keeps both CTAs (their
+// shared memory and TMEM) alive until nothing in flight can touch them.  No
+// load uses multicast.
 
 constexpr int kPairStages = 6;
 constexpr int kPairStageBytes = 2 * kABytes;                // 16 KB A half + 16 KB B half
@@ -508,7 +513,6 @@ constexpr uint32_t kIdescPair = (2u << 4) | (1u << 7) | (1u << 10) |
 
 struct __align__(8) PairBarriers {
     uint64_t full[kPairStages];
-    uint64_t peer_full[kPairStages];
     uint64_t empty[kPairStages];
     uint64_t acc_full[2];
     uint64_t acc_empty[2];
@@ -534,6 +538,18 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
                      cluster_addr)
                  : "memory");
+}
+
+// TMA load of one 128-row x 128-byte tile (rows y .. y+127 of the workspace
+// view) into this CTA's shared memory, completing on the barrier at the
+// shared::cluster address `bar` (the even CTA's)
+__device__ __forceinline__ void tma_tile_pair(uint32_t dst, const CUtensorMap* map, int32_t y,
+                                              uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(bar)
+        : "memory");
 }
 
 __device__ __forceinline__ void cluster_sync_all() {
@@ -572,7 +588,8 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     k_oz_gemm_pair(const FsOzProblem* __restrict__ probs, int64_t n_probs,
                    const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
-                   int chunk_ktiles, int32_t* flag) {
+                   int chunk_ktiles, int32_t* flag, const __grid_constant__ CUtensorMap ws_map,
+                   const int8_t* ws_base) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -586,7 +603,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < kPairStages; ++s) {
             mbar_init(smem_addr(&bars->full[s]), 1);
-            mbar_init(smem_addr(&bars->peer_full[s]), 1);
             mbar_init(smem_addr(&bars->empty[s]), 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -636,14 +652,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                                     break;
                                 }
                                 const uint32_t full = smem_addr(&bars->full[stage]);
-                                mbar_expect_tx(full, kPairStageBytes);
+                                if (rank == 0) mbar_expect_tx(full, 2 * kPairStageBytes);
                                 const int8_t* a = p.a_slices + s * a_slice +
                                                   (static_cast<int64_t>(kt) * p.a_rowtiles + a_rt) * kABytes;
                                 const int8_t* b = p.b_slices + (d - s) * b_slice +
                                                   (static_cast<int64_t>(kt) * p.b_rowtiles + b_rt) * kABytes;
                                 const uint32_t dst = base + stage * kPairStageBytes;
-                                bulk_g2s(dst, a, kABytes, full);
-                                bulk_g2s(dst + kABytes, b, kABytes, full);
+                                const uint32_t full_even = map_to_rank(full, 0);
+                                tma_tile_pair(dst, &ws_map, static_cast<int32_t>((a - ws_base) >> 7),
+                                              full_even);
+                                tma_tile_pair(dst + kABytes, &ws_map,
+                                              static_cast<int32_t>((b - ws_base) >> 7), full_even);
                                 issued_mask |= 1u << stage;
                                 issued_parity = (issued_parity & ~(1u << stage)) | (phase << stage);
                                 if (++stage == kPairStages) {
@@ -655,7 +674,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     }
                 }
             }
-            for (int s = 0; s < kPairStages; ++s) {
+            // the even CTA's full barriers complete only when the copies of
+            // both CTAs have landed
+            for (int s = 0; rank == 0 && s < kPairStages; ++s) {
                 if (issued_mask & (1u << s)) {
                     if (!mbar_wait_drain(smem_addr(&bars->full[s]), (issued_parity >> s) & 1u))
                         *abort_flag = 1;
@@ -663,29 +684,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             }
         }
     } else if (warp == 1 && rank == 1) {
-        // ---------------------------- relay (odd CTA): stage s landed here
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            bool ok = true;
-            for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
-                const FsOzProblem p = probs[tiles[t].problem];
-                for (int d = nslices - 1; ok && d >= 0; --d) {
-                    const int64_t n_fill = static_cast<int64_t>(d + 1) * p.ktiles;
-                    for (int64_t f = 0; f < n_fill; ++f) {
-                        if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
-                            ok = false;
-                            break;
-                        }
-                        mbar_arrive_remote(map_to_rank(smem_addr(&bars->peer_full[stage]), 0));
-                        if (++stage == kPairStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
-                    }
-                }
-            }
-        }
+        // the odd CTA's warp 1 only shares the TMEM allocation
     } else if (warp == 1) {
         // ------------------------------------------ MMA issuer (even CTA)
         if (lane == 0) {
@@ -709,9 +708,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         uint32_t accumulate = 0;
                         for (int s = 0; ok && s <= d; ++s) {
                             for (int kt = k0; kt < k1; ++kt) {
-                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag) ||
-                                    !mbar_wait(smem_addr(&bars->peer_full[stage]), phase,
-                                               abort_flag)) {
+                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
                                     ok = false;
                                     break;
                                 }
@@ -895,13 +892,54 @@ extern "C" int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
     return fsb::launch_status();
 }
 
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+}  // namespace
+
 extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
                                   const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
-                                  int32_t chunk_ktiles, int32_t* d_flag, void* stream) {
+                                  int32_t chunk_ktiles, const void* d_workspace,
+                                  int64_t workspace_bytes, int32_t* d_flag, void* stream) {
     if (n_probs < 0 || n_tiles < 0 || chunk_ktiles < 1) return FS_ERR_INVALID_ARG;
     if (nslices < 1 || nslices > FS_OZAKI_MAX_SLICES) return FS_ERR_INVALID_ARG;
     if (n_tiles == 0) return FS_OK;
-    if (d_probs == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    if (d_probs == nullptr || d_tiles == nullptr || d_workspace == nullptr)
+        return FS_ERR_INVALID_ARG;
+    // the workspace is viewed as rows of 128 bytes: 16-byte aligned base, whole
+    // rows, and row indices that fit the 32-bit TMA coordinate
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 127u) != 0 || workspace_bytes < 128 * 128 ||
+        (workspace_bytes & 127) != 0 || (workspace_bytes >> 7) >= (1LL << 31))
+        return FS_ERR_INVALID_ARG;
+    EncodeTiledFn enc = encode_tiled();
+    if (enc == nullptr) return FS_ERR_UNSUPPORTED;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {128, static_cast<cuuint64_t>(workspace_bytes >> 7)};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {128, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(d_workspace), dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return FS_ERR_INVALID_ARG;
     const long long bound = static_cast<long long>(nslices) * chunk_ktiles * fsb::oz::kTileK *
                             127LL * 127LL;
     if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
@@ -920,7 +958,8 @@ extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
     const int64_t max_clusters = fsb::kNumSM / 2;
     const int clusters = static_cast<int>(n_tiles < max_clusters ? n_tiles : max_clusters);
     fsb::oz::k_oz_gemm_pair<<<2 * clusters, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
-        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
+        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag, map,
+        static_cast<const int8_t*>(d_workspace));
     return fsb::launch_status();
 }
 

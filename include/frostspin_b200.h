@@ -212,13 +212,16 @@ int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
 
 /*
  * The same GEMM on 256 x 256 output tiles computed by clusters of two CTAs
- * (tcgen05.mma.cta_group::2, each CTA loading half of every operand stage).
- * Tiles index 256-row blocks of C (tm) and 256-column blocks (tn); every
- * problem listed in d_tiles must have an even a_rowtiles.
+ * (tcgen05.mma.cta_group::2, each CTA loading half of every operand stage by
+ * TMA through a tensor map over the workspace).  Tiles index 256-row blocks
+ * of C (tm) and 256-column blocks (tn); every problem listed in d_tiles must
+ * have an even a_rowtiles.  d_workspace / workspace_bytes: the buffer holding
+ * every problem's slices (128-byte aligned, a multiple of 128 bytes).
  */
 int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
                        const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
-                       int32_t chunk_ktiles, int32_t* d_flag, void* stream);
+                       int32_t chunk_ktiles, const void* d_workspace,
+                       int64_t workspace_bytes, int32_t* d_flag, void* stream);
 
 /*
  * Grouped Ozaki GEMM that allocates nothing.  No counterpart in the reference.
