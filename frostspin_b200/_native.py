@@ -61,6 +61,21 @@ GEMM_TILE_DTYPE = np.dtype(
     [("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")]
 )
 
+SPLIT_REDUCE_DTYPE = np.dtype(
+    [
+        ("W", "<u8"),
+        ("C", "<u8"),
+        ("ldc", "<i8"),
+        ("slice", "<i8"),
+        ("nslices", "<i4"),
+        ("M", "<i4"),
+        ("N", "<i4"),
+        ("pad", "<i4"),
+        ("alpha", "<f8"),
+        ("beta", "<f8"),
+    ]
+)
+
 OZ_OPERAND_DTYPE = np.dtype(
     [
         ("src", "<u8"),
@@ -141,6 +156,7 @@ SIGNATURES = {
     "fs_grouped_dgemm": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
     "fs_thin_dgemm_shape": (ctypes.c_int, [_P, _P, _P]),
     "fs_grouped_dgemm_thin": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
+    "fs_splitk_reduce": (ctypes.c_int, [_P, _I64, _I64, _P]),
     "fs_ozaki_geometry": (ctypes.c_int, [_P, _P, _P, _P]),
     "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
@@ -197,7 +213,7 @@ CALL_COUNTS = {}
 
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
-    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1,
+    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2, "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
     "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1,
 }

@@ -311,3 +311,41 @@ extern "C" int fs_grouped_dgemm_thin(const FsGemmProblem* d_problems, int64_t n_
         d_problems, n_problems, d_tiles, n_tiles);
     return fsb::launch_status();
 }
+
+// ------------------------------------------------------------ split-K reduce
+// When a contraction has too few output tiles to fill the GPU, the host cuts
+// long-K sector problems into K chunks whose partial products go to a
+// workspace (slice j of an item at W + j * slice); this kernel sums the slices
+// in order (deterministic, no atomics) and applies alpha / beta into C.
+namespace fsb {
+
+__global__ void __launch_bounds__(256)
+    k_splitk_reduce(const FsSplitReduce* __restrict__ items, int64_t n_items) {
+    const int64_t it = blockIdx.y;
+    if (it >= n_items) return;
+    const FsSplitReduce r = items[it];
+    const int64_t n = static_cast<int64_t>(r.M) * r.N;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double v = 0.0;
+        for (int j = 0; j < r.nslices; ++j) v += __ldg(r.W + j * r.slice + e);
+        const int64_t i = e / r.N, c = e - i * r.N;
+        double* dst = r.C + i * r.ldc + c;
+        *dst = (r.beta == 0.0) ? r.alpha * v : fma(r.beta, *dst, r.alpha * v);
+    }
+}
+
+}  // namespace fsb
+
+extern "C" int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items,
+                                int64_t max_elems, void* stream) {
+    if (n_items < 0 || max_elems < 0) return FS_ERR_INVALID_ARG;
+    if (n_items == 0 || max_elems == 0) return FS_OK;
+    if (d_items == nullptr) return FS_ERR_INVALID_ARG;
+    if (n_items > 65535) return FS_ERR_TOO_LARGE;
+    const int64_t blocks = (max_elems + 255) / 256;
+    const int gx = static_cast<int>(blocks < 4 * fsb::kNumSM ? blocks : 4 * fsb::kNumSM);
+    fsb::k_splitk_reduce<<<dim3(gx, static_cast<unsigned>(n_items)), 256, 0,
+                           fsb::as_stream(stream)>>>(d_items, n_items);
+    return fsb::launch_status();
+}

@@ -232,7 +232,75 @@ def _tile_table(arr, tm, tn, ntile):
     return tiles[order]
 
 
+_SPLITK_CHUNK = 1024        # smallest K chunk of a split problem
+_SPLITK_TARGET_TILES = 3 * 148 * 2   # two waves of 3 CTAs per SM
+
+
+def _split_k(arr, tm, tn, ntile):
+    """Cut long-K problems of a launch that has too few output tiles into K
+    chunks writing partial products to a workspace; returns the new problem
+    table and tile counts, the reduction items and the workspace (or None
+    when the launch already fills the GPU)."""
+    total = int(ntile.sum())
+    if total == 0 or total >= _SPLITK_TARGET_TILES:
+        return None
+    factor = min(16, -(-_SPLITK_TARGET_TILES // total))
+    K = arr["K"].astype(np.int64)
+    ks = np.minimum(factor, K // _SPLITK_CHUNK)
+    split = ks >= 2
+    if not split.any():
+        return None
+    M = arr["M"].astype(np.int64)
+    N = arr["N"].astype(np.int64)
+    w_sizes = np.where(split, ks * M * N, 0)
+    w_off = np.concatenate([[0], np.cumsum(w_sizes)[:-1]])
+    work = torch.empty(max(int(w_sizes.sum()), 1), dtype=torch.float64, device=dev.device())
+    base = work.data_ptr()
+    rows, items = [], np.zeros(int(split.sum()), dtype=_native.SPLIT_REDUCE_DTYPE)
+    n_items = 0
+    for i in range(arr.size):
+        if not split[i]:
+            rows.append(arr[i : i + 1])
+            continue
+        k_i, n_chunks = int(K[i]), int(ks[i])
+        chunk = -(-k_i // n_chunks)
+        chunk = -(-chunk // 16) * 16
+        starts = np.arange(0, k_i, chunk)
+        sub = np.repeat(arr[i : i + 1], starts.size)
+        a_step = int(arr["lda"][i]) if arr["transA"][i] else 1
+        b_step = 1 if arr["transB"][i] else int(arr["ldb"][i])
+        sub["A"] = arr["A"][i] + (8 * starts * a_step).astype(np.uint64)
+        sub["B"] = arr["B"][i] + (8 * starts * b_step).astype(np.uint64)
+        sub["K"] = np.minimum(chunk, k_i - starts)
+        sub["C"] = np.uint64(base) + (8 * (w_off[i] + np.arange(starts.size) * M[i] * N[i])).astype(np.uint64)
+        sub["ldc"] = N[i]
+        sub["alpha"] = 1.0
+        sub["beta"] = 0.0
+        rows.append(sub)
+        items[n_items] = (base + 8 * int(w_off[i]), arr["C"][i], arr["ldc"][i], M[i] * N[i],
+                          starts.size, M[i], N[i], 0, arr["alpha"][i], arr["beta"][i])
+        n_items += 1
+    new = np.concatenate(rows)
+    nt = ((new["M"].astype(np.int64) + tm - 1) // tm) * ((new["N"].astype(np.int64) + tn - 1) // tn)
+    return new, nt, items[:n_items], work
+
+
 def _dgemm(arr, problems, tm, tn, ntile):
+    sk = _split_k(arr, tm, tn, ntile)
+    if sk is not None:
+        arr, ntile, items, work = sk
+        tiles = _tile_table(arr, tm, tn, ntile)
+        d_prob = dev.upload(arr)
+        d_tiles = dev.upload(tiles)
+        _native.call("fs_grouped_dgemm", d_prob.data_ptr(), arr.size, d_tiles.data_ptr(),
+                     tiles.size, dev.stream())
+        d_items = dev.upload(items)
+        max_elems = int((items["M"].astype(np.int64) * items["N"]).max())
+        for start in range(0, items.size, 65535):
+            cnt = min(65535, items.size - start)
+            _native.call("fs_splitk_reduce", d_items.data_ptr() + start * items.itemsize, cnt,
+                         max_elems, dev.stream())
+        return d_prob, d_tiles, work
     tiles = _tile_table(arr, tm, tn, ntile)
     d_prob = dev.upload(arr)
     d_tiles = dev.upload(tiles)

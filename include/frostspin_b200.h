@@ -146,6 +146,27 @@ int fs_thin_dgemm_shape(int32_t* max_m, int32_t* max_k, int32_t* tile_n);
 int fs_grouped_dgemm_thin(const FsGemmProblem* d_problems, int64_t n_problems,
                           const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
 
+/*
+ * Split-K completion: C = alpha * sum_{j < nslices} W[j * slice ...] + beta * C
+ * for M x N row-major results (C leading dimension ldc, slices contiguous
+ * M x N), summed in slice order.  The host cuts a long-K sector problem into
+ * K chunks (each an FsGemmProblem writing slice j with alpha 1, beta 0) when a
+ * contraction has too few output tiles to fill the GPU.
+ */
+typedef struct FsSplitReduce {
+    const double* W;
+    double* C;
+    int64_t ldc;
+    int64_t slice;      /* elements between consecutive slices */
+    int32_t nslices;
+    int32_t M, N;
+    int32_t pad;
+    double alpha, beta;
+} FsSplitReduce;
+
+int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items, int64_t max_elems,
+                     void* stream);
+
 /* ------------------------------------- grouped GEMM on tcgen05 (Ozaki int8) */
 /*
  * FP64-class GEMM on the int8 tensor cores (tcgen05.mma kind::i8): every row of

@@ -82,6 +82,9 @@ int main(void) {
   F(FsOzProblem, N) F(FsOzProblem, K) F(FsOzProblem, a_rowtiles) F(FsOzProblem, b_rowtiles)
   F(FsOzProblem, ktiles) F(FsOzProblem, alpha) F(FsOzProblem, beta)
   S(FsOzTile) F(FsOzTile, problem) F(FsOzTile, tm) F(FsOzTile, tn)
+  S(FsSplitReduce) F(FsSplitReduce, W) F(FsSplitReduce, C) F(FsSplitReduce, ldc)
+  F(FsSplitReduce, slice) F(FsSplitReduce, nslices) F(FsSplitReduce, M)
+  F(FsSplitReduce, N) F(FsSplitReduce, alpha) F(FsSplitReduce, beta)
   return 0;
 }
 """
@@ -97,6 +100,7 @@ DTYPES = {
     "FsOzOperand": _native.OZ_OPERAND_DTYPE,
     "FsOzProblem": _native.OZ_PROBLEM_DTYPE,
     "FsOzTile": _native.OZ_TILE_DTYPE,
+    "FsSplitReduce": _native.SPLIT_REDUCE_DTYPE,
 }
 
 
