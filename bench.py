@@ -486,7 +486,7 @@ def run_ctmrg(args, world, rank, local):
         "gpu_launches": lmx if headline_mixed else l64,
         "clocks": clkmx if headline_mixed else clk64,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if args.symmetry == "u1":
             t_cpu, info = cpu_ctmrg_seconds(tensors, ctm_mixed, args.chi)
             info["value"] = 1.0 / t_cpu
