@@ -274,9 +274,12 @@ __global__ void __launch_bounds__(kThinThreads)
         const int n0 = tile.tn * kCols;
         if (n0 >= p.N) continue;
         __syncthreads();  // previous tile's reads of su are done
-        for (int i = threadIdx.x; i < kThinMax * kThinMax; i += kThinThreads) {
-            const int m = i / kThinMax, k = i % kThinMax;
-            su[i] = (m < p.M && k < p.K) ? p.A[static_cast<int64_t>(m) * p.lda + k] : 0.0;
+        // only the M x K entries are staged (rows beyond M are never read, and
+        // the k loop stops at K)
+        const int mk = p.M * p.K;
+        for (int i = threadIdx.x; i < mk; i += kThinThreads) {
+            const int m = i / p.K, k = i - m * p.K;
+            su[m * kThinMax + k] = p.A[static_cast<int64_t>(m) * p.lda + k];
         }
         __syncthreads();
         if (p.M <= 4)

@@ -186,11 +186,12 @@ def grouped_dgemm_table(arr, region="gemm_fp64"):
             _dgemm(sub, None, tm, tn, ntile)
 
 
-# rates of the two paths on B200 (int8: k_oz_gemm inside the SU(2) CTMRG
-# workload; FP64: the DMMA tile kernel on large sectors), used only to decide
-# which path a sector GEMM takes in a mixed-precision run
-_INT8_OPS = 1.3e15
-_FP64_FLOPS = 2.8e13
+# rates of the two paths on B200 inside the SU(2) CTMRG workload (int8: the
+# CTA-pair k_oz_gemm_pair; FP64: k_grouped_dgemm averaged over the sector
+# shapes it receives), used only to decide which path a sector GEMM takes in a
+# mixed-precision run
+_INT8_OPS = 1.8e15
+_FP64_FLOPS = 2.0e13
 _EPILOGUE_BPS = 2.0e12
 _SPLIT_BPS = 3.0e12
 
