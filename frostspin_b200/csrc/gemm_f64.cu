@@ -85,6 +85,37 @@ __device__ __forceinline__ void load_stage(const FsGemmProblem& p, int m0, int n
     }
 }
 
+// The DMMAs of one staged k slice for one warp's 32x32 block: k steps at or
+// beyond k_left, fragment rows at or beyond rows_left and fragment columns at
+// or beyond cols_left (all warp-uniform) are skipped.
+template <bool TA, bool TB>
+__device__ __forceinline__ void mma_slice(double (&acc)[4][4][2], const double* sa,
+                                          const double* sb, int k_left, int rows_left,
+                                          int cols_left) {
+    constexpr int a_step_i = TA ? 8 : 8 * kLdK;   // next fragment row block
+    constexpr int a_step_k = TA ? 4 * kLdR : 4;   // next k-step
+    constexpr int b_step_j = TB ? 8 * kLdK : 8;
+    constexpr int b_step_k = TB ? 4 : 4 * kLdR;
+#pragma unroll
+    for (int ks = 0; ks < kTK / 4; ++ks) {
+        if (ks * 4 >= k_left) break;
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = sa[ks * a_step_k + i * a_step_i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = sb[ks * b_step_k + j * b_step_j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (i * 8 >= rows_left) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j * 8 >= cols_left) break;
+                dmma(acc[i][j], a[i], b[j]);
+            }
+        }
+    }
+}
+
 // One 64x64 output tile: the cp.async pipeline over k and the DMMA fragments.
 template <bool TA, bool TB>
 __device__ __forceinline__ void dgemm_tile(const FsGemmProblem& p, int m0, int n0,
@@ -105,10 +136,6 @@ __device__ __forceinline__ void dgemm_tile(const FsGemmProblem& p, int m0, int n
     // per-thread fragment offsets inside a stage (k = 0)
     const int a_off = TA ? fk * kLdR + wm + fr : (wm + fr) * kLdK + fk;
     const int b_off = TB ? (wn + fr) * kLdK + fk : fk * kLdR + wn + fr;
-    constexpr int a_step_i = TA ? 8 : 8 * kLdK;   // next fragment row block
-    constexpr int a_step_k = TA ? 4 * kLdR : 4;   // next k-step
-    constexpr int b_step_j = TB ? 8 * kLdK : 8;
-    constexpr int b_step_k = TB ? 4 : 4 * kLdR;
 
     const int nk = (p.K + kTK - 1) / kTK;
     __syncthreads();  // every warp is done with the previous tile's stages
@@ -128,18 +155,9 @@ __device__ __forceinline__ void dgemm_tile(const FsGemmProblem& p, int m0, int n
         }
         const double* sa = smem + (kt % kStages) * kStageDoubles + a_off;
         const double* sb = smem + (kt % kStages) * kStageDoubles + kOpTile + b_off;
-#pragma unroll
-        for (int ks = 0; ks < kTK / 4; ++ks) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = sa[ks * a_step_k + i * a_step_i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = sb[ks * b_step_k + j * b_step_j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
-        }
+        // the full padded slice: at 168 registers this kernel has no room for
+        // the edge tests (the streaming kernel skips padded fragments)
+        mma_slice<TA, TB>(acc, sa, sb, kTK, kTM, kTN);
     }
     cp_async_wait<0>();
 
@@ -181,6 +199,128 @@ __global__ void __launch_bounds__(kGemmThreads, 3)
     }
 }
 
+// Streaming variant for launches whose problems share both transpose flags,
+// used for short-K sector products (wide recouplings and projector
+// applications with K of a few tens): one cp.async ring runs continuously
+// across the CTA's tiles, so the first k slices of the next tile load while
+// the current tile finishes and writes its outputs, and fragments or k steps
+// wholly outside the problem (M, N, K padding of the 64x64x16 tiling) issue no
+// DMMA.  Tiles of problems with K = 0 consume no stage (their output is
+// beta * C).
+struct TileCursor {
+    int64_t t;
+    FsGemmProblem p;
+    int m0, n0, nk;
+};
+
+__device__ __forceinline__ bool cursor_seek(TileCursor& c, int64_t t,
+                                            const FsGemmProblem* __restrict__ problems,
+                                            int64_t n_problems,
+                                            const FsGemmTile* __restrict__ tiles, int64_t n_tiles,
+                                            bool need_k) {
+    for (; t < n_tiles; t += gridDim.x) {
+        const FsGemmTile tile = tiles[t];
+        if (tile.problem < 0 || tile.problem >= n_problems) continue;
+        c.p = problems[tile.problem];
+        c.m0 = tile.tm * kTM;
+        c.n0 = tile.tn * kTN;
+        if (c.m0 >= c.p.M || c.n0 >= c.p.N) continue;
+        c.nk = (c.p.K + kTK - 1) / kTK;
+        if (need_k && c.nk == 0) continue;
+        c.t = t;
+        return true;
+    }
+    c.t = n_tiles;
+    return false;
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(kGemmThreads, 3)
+    k_grouped_dgemm_stream(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
+                           const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
+    extern __shared__ __align__(16) double smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wm = (warp & 1) * 32;
+    const int wn = (warp >> 1) * 32;
+    const int fr = lane >> 2;
+    const int fk = lane & 3;
+    const int a_off = TA ? fk * kLdR + wm + fr : (wm + fr) * kLdK + fk;
+    const int b_off = TB ? (wn + fr) * kLdK + fk : fk * kLdR + wn + fr;
+
+    // loader: the next (tile, k slice) to fetch; tiles without k slices skipped
+    TileCursor ld;
+    bool ld_ok = cursor_seek(ld, blockIdx.x, problems, n_problems, tiles, n_tiles, true);
+    int ld_k = 0;
+    int64_t issued = 0;
+    auto issue = [&]() {
+        if (ld_ok) {
+            load_stage<TA, TB>(ld.p, ld.m0, ld.n0, ld_k * kTK,
+                               smem + (issued % kStages) * kStageDoubles);
+            ++issued;
+            if (++ld_k == ld.nk) {
+                ld_k = 0;
+                ld_ok = cursor_seek(ld, ld.t + gridDim.x, problems, n_problems, tiles, n_tiles,
+                                    true);
+            }
+        }
+        cp_async_commit();
+    };
+
+    // consumer: every tile of this CTA in order (K = 0 tiles included)
+    TileCursor cs;
+    bool cs_ok = cursor_seek(cs, blockIdx.x, problems, n_problems, tiles, n_tiles, false);
+    int cs_k = 0;
+    int64_t consumed = 0;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) issue();
+
+    while (cs_ok) {
+        if (cs_k < cs.nk) {
+            // stage `consumed` is the consumed-th issued one: its group is
+            // complete once at most kStages - 2 newer groups are pending
+            cp_async_wait<kStages - 2>();
+            __syncthreads();  // and every warp is done with the slot refilled next
+            issue();
+            const double* sa = smem + (consumed % kStages) * kStageDoubles + a_off;
+            const double* sb = smem + (consumed % kStages) * kStageDoubles + kOpTile + b_off;
+            mma_slice<TA, TB>(acc, sa, sb, cs.p.K - cs_k * kTK, cs.p.M - (cs.m0 + wm),
+                              cs.p.N - (cs.n0 + wn));
+            ++consumed;
+            ++cs_k;
+        }
+        if (cs_k < cs.nk) continue;
+        // tile done: write it while the next tile's first slices load
+        const FsGemmProblem& p = cs.p;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gi = cs.m0 + wm + i * 8 + fr;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int gj = cs.n0 + wn + j * 8 + fk * 2 + h;
+                    if (gi < p.M && gj < p.N) {
+                        double* c = p.C + static_cast<int64_t>(gi) * p.ldc + gj;
+                        const double v = p.alpha * acc[i][j][h];
+                        *c = (p.beta == 0.0) ? v : fma(p.beta, *c, v);
+                    }
+                    acc[i][j][h] = 0.0;
+                }
+            }
+        }
+        cs_k = 0;
+        cs_ok = cursor_seek(cs, cs.t + gridDim.x, problems, n_problems, tiles, n_tiles, false);
+    }
+    cp_async_wait<0>();
+}
+
 }  // namespace fsb
 
 extern "C" int fs_dgemm_tile_shape(int32_t* tile_m, int32_t* tile_n) {
@@ -207,6 +347,42 @@ extern "C" int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_probl
     fsb::k_grouped_dgemm<<<grid, fsb::kGemmThreads, fsb::kGemmSmem, fsb::as_stream(stream)>>>(
         d_problems, n_problems, d_tiles, n_tiles);
     return fsb::launch_status();
+}
+
+namespace {
+
+template <bool TA, bool TB>
+int launch_stream(const FsGemmProblem* d_problems, int64_t n_problems, const FsGemmTile* d_tiles,
+                  int64_t n_tiles, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(fsb::k_grouped_dgemm_stream<TA, TB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(fsb::kGemmSmem)) != cudaSuccess)
+            return fsb::launch_status();
+        configured = true;
+    }
+    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 3;
+    const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
+    fsb::k_grouped_dgemm_stream<TA, TB><<<grid, fsb::kGemmThreads, fsb::kGemmSmem, s>>>(
+        d_problems, n_problems, d_tiles, n_tiles);
+    return fsb::launch_status();
+}
+
+}  // namespace
+
+extern "C" int fs_grouped_dgemm_uniform(const FsGemmProblem* d_problems, int64_t n_problems,
+                                        const FsGemmTile* d_tiles, int64_t n_tiles,
+                                        int32_t trans_a, int32_t trans_b, void* stream) {
+    if (n_tiles < 0 || n_problems < 0) return FS_ERR_INVALID_ARG;
+    if (n_tiles == 0) return FS_OK;
+    if (d_problems == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    cudaStream_t s = fsb::as_stream(stream);
+    if (trans_a)
+        return trans_b ? launch_stream<true, true>(d_problems, n_problems, d_tiles, n_tiles, s)
+                       : launch_stream<true, false>(d_problems, n_problems, d_tiles, n_tiles, s);
+    return trans_b ? launch_stream<false, true>(d_problems, n_problems, d_tiles, n_tiles, s)
+                   : launch_stream<false, false>(d_problems, n_problems, d_tiles, n_tiles, s);
 }
 
 // ---------------------------------------------------------------- thin GEMMs

@@ -286,6 +286,24 @@ def _split_k(arr, tm, tn, ntile):
     return new, nt, items[:n_items], work
 
 
+_STREAM_MAX_K = 256   # longest K of a launch that goes to the streaming kernel
+
+
+def _launch_dgemm(arr, d_prob, d_tiles, n_tiles):
+    """One DMMA launch over a problem table: the streaming kernel when every
+    problem has the same transpose flags and a short K (pipeline fill and
+    padded fragments dominate there), else the per-tile kernel (faster on long
+    K, where it keeps a few registers more for the DMMA loop)."""
+    ta, tb = arr["transA"], arr["transB"]
+    if (arr.size and (ta == ta[0]).all() and (tb == tb[0]).all()
+            and int(arr["K"].max()) <= _STREAM_MAX_K):
+        _native.call("fs_grouped_dgemm_uniform", d_prob.data_ptr(), arr.size,
+                     d_tiles.data_ptr(), n_tiles, int(ta[0]), int(tb[0]), dev.stream())
+    else:
+        _native.call("fs_grouped_dgemm", d_prob.data_ptr(), arr.size, d_tiles.data_ptr(),
+                     n_tiles, dev.stream())
+
+
 def _dgemm(arr, problems, tm, tn, ntile):
     sk = _split_k(arr, tm, tn, ntile)
     if sk is not None:
@@ -293,8 +311,7 @@ def _dgemm(arr, problems, tm, tn, ntile):
         tiles = _tile_table(arr, tm, tn, ntile)
         d_prob = dev.upload(arr)
         d_tiles = dev.upload(tiles)
-        _native.call("fs_grouped_dgemm", d_prob.data_ptr(), arr.size, d_tiles.data_ptr(),
-                     tiles.size, dev.stream())
+        _launch_dgemm(arr, d_prob, d_tiles, tiles.size)
         d_items = dev.upload(items)
         max_elems = int((items["M"].astype(np.int64) * items["N"]).max())
         for start in range(0, items.size, 65535):
@@ -305,14 +322,7 @@ def _dgemm(arr, problems, tm, tn, ntile):
     tiles = _tile_table(arr, tm, tn, ntile)
     d_prob = dev.upload(arr)
     d_tiles = dev.upload(tiles)
-    _native.call(
-        "fs_grouped_dgemm",
-        d_prob.data_ptr(),
-        arr.size,
-        d_tiles.data_ptr(),
-        tiles.size,
-        dev.stream(),
-    )
+    _launch_dgemm(arr, d_prob, d_tiles, tiles.size)
     return d_prob, d_tiles
 
 

@@ -135,6 +135,16 @@ int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_problems,
                      const FsGemmTile* d_tiles, int64_t n_tiles, void* stream);
 
 /*
+ * The same launch when every problem has transA == trans_a and transB ==
+ * trans_b (the caller guarantees it): one cp.async ring runs across each CTA's
+ * tiles, so the next tile's first k slices load while the current tile writes
+ * its outputs.  Same call sites as fs_grouped_dgemm.
+ */
+int fs_grouped_dgemm_uniform(const FsGemmProblem* d_problems, int64_t n_problems,
+                             const FsGemmTile* d_tiles, int64_t n_tiles, int32_t trans_a,
+                             int32_t trans_b, void* stream);
+
+/*
  * Thin problems of the same table format: M <= max_m, K <= max_k, both
  * operands row-major (transA == transB == 0), N large -- the recoupling
  * products of the SU(2) permute (frostspin/symmetric_tensor/

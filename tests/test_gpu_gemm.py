@@ -52,14 +52,83 @@ def test_grouped_dgemm_beta_accumulates():
     run_table(SHAPES[:6], True, False, -2.0)
 
 
+def _delta(before, name):
+    from frostspin_b200 import _native
+
+    return _native.CALL_COUNTS.get(name, 0) - before.get(name, 0)
+
+
 def test_thin_and_tile_kernels_both_launch():
     from frostspin_b200 import _native
 
     before = dict(_native.CALL_COUNTS)
     run_table([(4, 5000, 4), (100, 100, 100)], False, False, 0.0)
-    after = _native.CALL_COUNTS
-    assert after.get("fs_grouped_dgemm_thin", 0) - before.get("fs_grouped_dgemm_thin", 0) == 1
-    assert after.get("fs_grouped_dgemm", 0) - before.get("fs_grouped_dgemm", 0) == 1
+    assert _delta(before, "fs_grouped_dgemm_thin") == 1
+    # one transpose combination in the table: the streaming DMMA kernel
+    assert _delta(before, "fs_grouped_dgemm_uniform") == 1
+    assert _delta(before, "fs_grouped_dgemm") == 0
+
+
+SHORT_K = [  # (M, N, K): wide short-K sectors, ragged in every dimension
+    (64, 64, 16), (65, 63, 17), (130, 257, 129), (33, 300, 31), (263, 5000, 82),
+    (98, 3000, 19), (217, 4100, 58), (40, 70, 0), (7, 9, 3), (200, 3, 256),
+]
+
+
+@pytest.mark.parametrize("trans_a", [False, True])
+@pytest.mark.parametrize("trans_b", [False, True])
+def test_streaming_kernel_short_k(trans_a, trans_b):
+    """Launches with one transpose combination and K <= 256 run the streaming
+    kernel (cp.async ring across tiles, padded fragments skipped)."""
+    from frostspin_b200 import _native
+
+    before = dict(_native.CALL_COUNTS)
+    run_table(SHORT_K, trans_a, trans_b, 0.0)
+    run_table(SHORT_K, trans_a, trans_b, -0.5)
+    assert _delta(before, "fs_grouped_dgemm_uniform") == 2
+    assert _delta(before, "fs_grouped_dgemm") == 0
+
+
+def test_long_k_uses_per_tile_kernel():
+    from frostspin_b200 import _native
+
+    before = dict(_native.CALL_COUNTS)
+    run_table([(100, 100, 300), (64, 64, 64)], False, False, 0.0)
+    assert _delta(before, "fs_grouped_dgemm") == 1
+    assert _delta(before, "fs_grouped_dgemm_uniform") == 0
+
+
+def test_mixed_transposes_in_one_launch():
+    """Problems with different transpose flags share one launch of the
+    per-tile kernel (the streaming kernel needs uniform flags)."""
+    import torch
+
+    from frostspin_b200 import _native, linalg
+
+    rng = np.random.default_rng(5)
+    shapes = [(65, 63, 17), (130, 257, 129), (200, 3, 500), (16, 16, 0), (64, 64, 64)]
+    arr = np.zeros(len(shapes), dtype=_native.GEMM_PROBLEM_DTYPE)
+    keep, refs, outs = [], [], []
+    for i, (M, N, K) in enumerate(shapes):
+        ta, tb = i % 2 == 1, i % 3 == 1
+        A = rng.standard_normal((M, K))
+        B = rng.standard_normal((K, N))
+        dA = torch.from_numpy(np.ascontiguousarray(A.T if ta else A)).cuda()
+        dB = torch.from_numpy(np.ascontiguousarray(B.T if tb else B)).cuda()
+        dC = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+        keep += [dA, dB]
+        outs.append(dC)
+        refs.append((A @ B, np.abs(A).sum(axis=1)[:, None] * np.abs(B).max(initial=0.0)))
+        arr[i] = (dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M if ta else K, K if tb else N,
+                  N, M, N, K, int(ta), int(tb), 0, 1.0, 0.0)
+    before = dict(_native.CALL_COUNTS)
+    linalg.grouped_dgemm_table(arr)
+    torch.cuda.synchronize()
+    assert _delta(before, "fs_grouped_dgemm") == 1
+    assert _delta(before, "fs_grouped_dgemm_uniform") == 0
+    for (ref, scale), dC in zip(refs, outs, strict=True):
+        got = dC.cpu().numpy()
+        assert np.all(np.abs(got - ref) <= 1e-14 * (scale + 1.0) * 4 + 1e-15)
 
 
 @pytest.mark.parametrize("trans_a", [False, True])

@@ -187,5 +187,6 @@ def test_su2_native_kernels_launched():
     after = _native.CALL_COUNTS
     assert after.get("fs_abelian_permute", 0) - before.get("fs_abelian_permute", 0) == 2
     gemms = sum(after.get(k, 0) - before.get(k, 0)
-                for k in ("fs_grouped_dgemm", "fs_grouped_dgemm_thin"))
+                for k in ("fs_grouped_dgemm", "fs_grouped_dgemm_uniform",
+                          "fs_grouped_dgemm_thin"))
     assert 1 <= gemms <= 2  # thin groups and tiled groups, one launch each
