@@ -582,6 +582,86 @@ def case_su2():
     save("su2", data)
 
 
+def _o2_pack_all(name, t, perms, data):
+    """An O(2) tensor with its dense form, its U(1) cast, a list of permutes
+    (each with its dense form and U(1) cast) and its transpose."""
+    pack_tensor(name, t, data)
+    data[name + "_dense"] = t.toarray()
+    pack_tensor(name + "_u1", t.toU1(), data)
+    for i, (ra, ca) in enumerate(perms):
+        p = t.permute(ra, ca)
+        pre = f"{name}_perm{i}"
+        pack_tensor(pre, p, data)
+        pack_tensor(pre + "_u1", p.toU1(), data)
+        data[pre + "_axes"] = np.array(ra + ca)
+        data[pre + "_nrr"] = np.array(len(ra))
+        data[pre + "_dense"] = p.toarray()
+    tt = t.transpose()
+    pack_tensor(name + "_transpose", tt, data)
+    data[name + "_transpose_dense"] = tt.toarray()
+
+
+def case_o2():
+    """O(2) fixtures.  The inputs of the reference's tests/test_o2_tensor.py
+    (representations r1..r7, seed 42, the pathological tensors with the 0odd,
+    0even or both blocks removed, only doublets, only odd or only even fixed
+    points in the columns), plus a random tensor with a mixed signature, each
+    permuted in several ways, transposed and cast to U(1)."""
+    from frostspin import O2SymmetricTensor
+
+    data = {}
+    rng = np.random.default_rng(42)
+    r1 = np.array([[1, 1, 1, 1], [-1, 0, 1, 2]])
+    r2 = np.array([[2, 1, 1, 1], [-1, 0, 1, 2]])
+    r3 = np.array([[1, 2, 1, 1], [-1, 0, 1, 2]])
+    r4 = np.array([[1, 1, 1, 1], [-1, 0, 2, 3]])
+    r5 = np.array([[2, 1, 1, 1], [-1, 0, 2, 3]])
+    perms = [((2, 1, 4), (0, 3)), ((0, 1, 3), (2, 4)), ((4,), (3, 2, 1, 0)),
+             ((3, 0, 4, 1), (2,))]
+    t = O2SymmetricTensor.random((r1, r2, r3), (r4, r5), rng=rng)
+    t /= t.norm()
+    _o2_pack_all("base", t, perms, data)
+    data["base_norm"] = np.array(t.norm())
+    pack_tensor("base_dagger", t.dagger(), data)
+    m = t @ t.dagger()
+    pack_tensor("base_matmul", m, data)
+
+    z = t.copy()
+    z.blocks[0][:] = 0
+    no_odd = O2SymmetricTensor(z.row_reps, z.col_reps, z.blocks[1:], z.block_irreps[1:],
+                               z.signature)
+    _o2_pack_all("noodd", no_odd, perms[:2], data)
+    z = t.copy()
+    no_even = O2SymmetricTensor(z.row_reps, z.col_reps, z.blocks[:1] + z.blocks[2:],
+                                (-1, *z.block_irreps[2:]), z.signature)
+    _o2_pack_all("noeven", no_even, perms[:2], data)
+    z = t.copy()
+    no_zero = O2SymmetricTensor(z.row_reps, z.col_reps, z.blocks[2:], z.block_irreps[2:],
+                                z.signature)
+    _o2_pack_all("nozero", no_zero, perms[:2], data)
+    z = t.copy()
+    only_zero = O2SymmetricTensor(z.row_reps, z.col_reps, z.blocks[:2], z.block_irreps[:2],
+                                  z.signature)
+    _o2_pack_all("onlyzero", only_zero, perms[:2], data)
+
+    for name, r6, r7 in (
+        ("doublets", np.array([[1, 1, 1], [2, 3, 4]]), np.array([[2, 1], [2, 3]])),
+        ("oddfix", np.array([[4], [-1]]), np.array([[5], [-1]])),
+        ("evenfix", np.array([[4], [0]]), np.array([[5], [0]])),
+    ):
+        t2 = O2SymmetricTensor.random((r1, r2, r6), (r3, r7), rng=rng)
+        t2 /= t2.norm()
+        _o2_pack_all(name, t2, [((0, 1, 3), (2, 4)), ((4, 2), (1, 0, 3))], data)
+
+    rng = np.random.default_rng(5)
+    sig = np.array([0, 1, 1, 0], dtype=bool)
+    ra = np.array([[1, 2, 1], [-1, 0, 1]])
+    rb = np.array([[1, 1, 2], [0, 1, 2]])
+    t4 = O2SymmetricTensor.random((ra, rb), (rb, ra), signature=sig, rng=rng)
+    _o2_pack_all("sig", t4, [((0, 2), (1, 3)), ((3,), (0, 1, 2)), ((1, 2, 3), (0,))], data)
+    save("o2", data)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
