@@ -9,6 +9,7 @@ Device-resident SymmetricTensor types mirror the interface of frostspin 1.0.0
 from .linalg import gemm_precision, gemm_precision_mode, set_gemm_precision
 from .symmetric_tensor import (
     DiagonalTensor,
+    O2SymmetricTensor,
     SU2SymmetricTensor,
     U1SymmetricTensor,
     get_symmetric_tensor_type,
@@ -18,6 +19,7 @@ __version__ = "0.1.0"
 
 __all__ = [
     "DiagonalTensor",
+    "O2SymmetricTensor",
     "SU2SymmetricTensor",
     "U1SymmetricTensor",
     "gemm_precision",

@@ -127,6 +127,31 @@ PAIR_BLOCK_DTYPE = np.dtype(
     ]
 )
 
+FS_O2_MAXTERMS = 4
+
+O2_TERM_DTYPE = np.dtype(
+    [
+        ("src_off", "<i8"),
+        ("rs", "<i8"),
+        ("cs", "<i8"),
+        ("ridx_off", "<i8"),
+        ("cidx_off", "<i8"),
+        ("rcoef_off", "<i8"),
+        ("ccoef_off", "<i8"),
+    ]
+)
+
+O2_BLOCK_DTYPE = np.dtype(
+    [
+        ("out_off", "<i8"),
+        ("nrows", "<i8"),
+        ("ncols", "<i8"),
+        ("nterms", "<i4"),
+        ("pad", "<i4"),
+        ("terms", O2_TERM_DTYPE, (FS_O2_MAXTERMS,)),
+    ]
+)
+
 DIAG_BLOCK_DTYPE = np.dtype(
     [
         ("x_off", "<i8"),
@@ -172,6 +197,7 @@ SIGNATURES = {
     "fs_weighted_sum": (ctypes.c_int, [_P, _P, _I64, _P, _I64, _P, _P]),
     "fs_pair_contract": (ctypes.c_int, [_P, _P, _P, _I64, _P, _I64, _P, _P]),
     "fs_diag_mul": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
+    "fs_o2_recombine": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _P, _I64, _P, _P]),
 }
 
 _lib = None
@@ -218,7 +244,7 @@ LAUNCHES_PER_CALL = {
     "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2,
     "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
-    "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1,
+    "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1, "fs_o2_recombine": 1,
 }
 
 

@@ -359,6 +359,44 @@ int fs_diag_mul(const double* d_x, const double* d_diag, double* d_out,
  * 2 exact special cases (DiagonalTensor.__pow__, diagonal_tensor.py:133-143). */
 int fs_pow(const double* d_x, double* d_y, int64_t n, double p, void* stream);
 
+/*
+ * O(2) <-> U(1) change of basis of symmetric-tensor blocks, replacing the
+ * reference's Sz-reflection and 0odd / 0even loops
+ * (frostspin/symmetric_tensor/o2_symmetric_tensor.py: _generate_neg_sz_blocks
+ * :798-851 with _numba_generate_refl_block :327-354, _numba_merge_b0oe
+ * :269-288, _numba_split_b0 :291-310; used by toU1 :682-733, from_U1 :650-675,
+ * _permute_data :853-936 and _transpose_data :938-942).
+ *
+ * Output block b (C-order, nrows x ncols at d_out + out_off) gets
+ *   out[i, j] = sum_t (coef[rcoef_off + i] * src[p_t(i, j)]) * coef[ccoef_off + j],
+ *   p_t(i, j) = src_off + index[ridx_off + i] * rs + index[cidx_off + j] * cs,
+ * summed over its nterms (<= FS_O2_MAXTERMS) terms in order, each product
+ * rounded separately.  Source and output positions outside [0, src_len) /
+ * [0, out_len) are skipped and reported in *d_flag (FS_ERR_BOUNDS, if d_flag
+ * is not null); the host tables are validated before the call.  max_rows is
+ * the largest nrows; at most 65535 blocks per call.
+ */
+#define FS_O2_MAXTERMS 4
+
+typedef struct FsO2Term {
+    int64_t src_off;
+    int64_t rs, cs;                  /* source row / column strides (elements) */
+    int64_t ridx_off, cidx_off;      /* into the index table                   */
+    int64_t rcoef_off, ccoef_off;    /* into the coefficient table             */
+} FsO2Term;
+
+typedef struct FsO2Block {
+    int64_t out_off;
+    int64_t nrows, ncols;
+    int32_t nterms;
+    int32_t pad;
+    FsO2Term terms[FS_O2_MAXTERMS];
+} FsO2Block;
+
+int fs_o2_recombine(const double* d_src, int64_t src_len, double* d_out, int64_t out_len,
+                    const FsO2Block* d_blocks, int64_t n_blocks, const int64_t* d_index,
+                    const double* d_coef, int64_t max_rows, int32_t* d_flag, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,10 @@ int main(void) {
   S(FsSplitReduce) F(FsSplitReduce, W) F(FsSplitReduce, C) F(FsSplitReduce, ldc)
   F(FsSplitReduce, slice) F(FsSplitReduce, nslices) F(FsSplitReduce, M)
   F(FsSplitReduce, N) F(FsSplitReduce, alpha) F(FsSplitReduce, beta)
+  S(FsO2Term) F(FsO2Term, src_off) F(FsO2Term, rs) F(FsO2Term, cs) F(FsO2Term, ridx_off)
+  F(FsO2Term, cidx_off) F(FsO2Term, rcoef_off) F(FsO2Term, ccoef_off)
+  S(FsO2Block) F(FsO2Block, out_off) F(FsO2Block, nrows) F(FsO2Block, ncols)
+  F(FsO2Block, nterms) F(FsO2Block, terms)
   return 0;
 }
 """
@@ -101,6 +105,8 @@ DTYPES = {
     "FsOzProblem": _native.OZ_PROBLEM_DTYPE,
     "FsOzTile": _native.OZ_TILE_DTYPE,
     "FsSplitReduce": _native.SPLIT_REDUCE_DTYPE,
+    "FsO2Term": _native.O2_TERM_DTYPE,
+    "FsO2Block": _native.O2_BLOCK_DTYPE,
 }
 
 
