@@ -105,6 +105,35 @@ def compute_fusion_tensor(rep1, rep2, s1, s2, *, max_irrep=2**30):
     return np.array([degen, irreps], dtype=np.int64), projector
 
 
+def _o2_leg(rep):
+    """O(2) representation of one SU(2) leg, the state order that takes the
+    leg to O(2) order and the sign of every state (su2_symmetric_tensor.py:
+    272-304).  States of a multiplet of dimension irr have 2 S_z = irr - 1,
+    irr - 3, ..., 1 - irr.  O(2) label: |2 S_z|, or -1 (0odd) for S_z = 0 when
+    irr = 3 mod 4.  Sign -1 for S_z < 0 with 2 S_z = irr + 1 (mod 4) for integer
+    spin, 2 S_z = irr - 1 (mod 4) for half-integer spin.  Order: label
+    ascending, then S_z descending, then multiplet order."""
+    sz, lab, neg = [], [], []
+    for d, irr in zip(np.asarray(rep[0]), np.asarray(rep[1]), strict=True):
+        irr = int(irr)
+        s = np.arange(irr - 1, -irr, -2, dtype=np.int64)
+        lb = np.abs(s)
+        if irr % 4 == 3:
+            lb[irr // 2] = -1
+        target = (irr + 1) % 4 if irr % 2 else (irr - 1) % 4
+        flip = (s < 0) & (s % 4 == target)
+        sz.append(np.tile(s, int(d)))
+        lab.append(np.tile(lb, int(d)))
+        neg.append(np.tile(flip, int(d)))
+    sz = np.concatenate(sz)
+    lab = np.concatenate(lab)
+    sign = 1.0 - 2.0 * np.concatenate(neg)
+    order = np.lexsort((-sz, lab))
+    irreps, degen = np.unique(lab, return_counts=True)
+    degen[irreps > 0] //= 2
+    return np.array([degen, irreps], dtype=np.int64), order, sign
+
+
 class SU2SymmetricTensor(LieGroupSymmetricTensor):
     """SU(2) SymmetricTensor (su2_symmetric_tensor.py:130-338)."""
 
@@ -193,7 +222,28 @@ class SU2SymmetricTensor(LieGroupSymmetricTensor):
         return out
 
     def toO2(self):
-        raise NotImplementedError("O(2) tensors are not part of this package")
+        """su2_symmetric_tensor.py:249-318, through the dense tensor as in the
+        reference.  Every leg is reordered into O(2) order (label |2 S_z|,
+        except S_z = 0 of an odd integer spin, which is 0odd; +n states before
+        -n states) and some S_z < 0 basis vectors change sign to follow the
+        O(2) reflection convention; the result is a gauge transform of the
+        tensor, invisible once legs are contracted."""
+        from .o2_symmetric_tensor import O2SymmetricTensor
+
+        arr = self.toarray()
+        o2_reps = []
+        for ax, r in enumerate(self._row_reps + self._col_reps):
+            rep, order, sign = _o2_leg(r)
+            o2_reps.append(rep)
+            shape = [1] * arr.ndim
+            shape[ax] = sign.size
+            arr = np.take(arr * sign.reshape(shape), order, axis=ax)
+        out = O2SymmetricTensor.from_array(arr, o2_reps[: self._nrr], o2_reps[self._nrr :],
+                                           self._signature)
+        if __debug__:
+            n1, n2 = self.norm(), out.norm()
+            assert abs(n1 - n2) <= 1e-13 * max(n1, 1.0)
+        return out
 
     # --------------------------------------------------- Clebsch-Gordan data
     @classmethod

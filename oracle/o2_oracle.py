@@ -337,3 +337,37 @@ def matmul(a, b):
     sig = np.r_[a.signature[: a.nrr], b.signature[b.nrr :]]
     return OTensor(a.row_reps, b.col_reps, [a.blocks[i] @ b.blocks[j] for i, j in
                                             zip(i1, i2, strict=True)], common, sig)
+
+
+def su2_leg_to_o2(rep):
+    """su2_symmetric_tensor.py:272-304 for one leg: O(2) representation, the
+    state order taking the leg to O(2) order and the sign of every state."""
+    sz, lab, sign = [], [], []
+    for d, irr in zip(rep[0], rep[1], strict=True):
+        irr = int(irr)
+        for _ in range(int(d)):
+            for s in range(irr - 1, -irr, -2):
+                lb = abs(s)
+                if s == 0 and irr % 4 == 3:
+                    lb = -1
+                flip = s < 0 and s % 4 == ((irr + 1) % 4 if irr % 2 else (irr - 1) % 4)
+                sz.append(s)
+                lab.append(lb)
+                sign.append(-1.0 if flip else 1.0)
+    order = sorted(range(len(sz)), key=lambda i: (lab[i], -sz[i], i))
+    irreps = sorted(set(lab))
+    degen = [lab.count(q) // (2 if q > 0 else 1) for q in irreps]
+    return np.array([degen, irreps]), np.array(order), np.array(sign)
+
+
+def from_su2_dense(arr, su2_row_reps, su2_col_reps, signature):
+    """SU2SymmetricTensor.toO2 (su2_symmetric_tensor.py:249-318) from the dense
+    SU(2) tensor: legs reordered and signed, then from_array."""
+    reps = []
+    for ax, r in enumerate(list(su2_row_reps) + list(su2_col_reps)):
+        rep, order, sign = su2_leg_to_o2(r)
+        reps.append(rep)
+        arr = np.moveaxis(np.moveaxis(arr, ax, 0)[order] * sign[order].reshape(
+            (-1,) + (1,) * (arr.ndim - 1)), 0, ax)
+    nrr = len(su2_row_reps)
+    return from_array(arr, reps[:nrr], reps[nrr:], signature)

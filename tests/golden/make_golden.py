@@ -659,6 +659,23 @@ def case_o2():
     rb = np.array([[1, 1, 2], [0, 1, 2]])
     t4 = O2SymmetricTensor.random((ra, rb), (rb, ra), signature=sig, rng=rng)
     _o2_pack_all("sig", t4, [((0, 2), (1, 3)), ((3,), (0, 1, 2)), ((1, 2, 3), (0,))], data)
+
+    # SU(2) -> O(2) casts (su2_symmetric_tensor.py:249-318): integer and
+    # half-integer spins up to spin 5/2, whose sign convention differs
+    from frostspin import SU2SymmetricTensor
+
+    rng = np.random.default_rng(9)
+    for name, rows, cols, sig in (
+        ("su2cast_int", (su2_rep([1, 2], [1, 3]), su2_rep([1, 1], [3, 5])),
+         (su2_rep([2, 1], [1, 3]), su2_rep([1], [5])), [0, 1, 1, 0]),
+        ("su2cast_half", (su2_rep([1, 1], [2, 4]), su2_rep([2], [2])),
+         (su2_rep([1, 1], [2, 4]), su2_rep([1, 1], [2, 6])), [0, 0, 1, 1]),
+        ("su2cast_mixed", (su2_rep([1, 1, 1], [2, 4, 6]),),
+         (su2_rep([1, 1], [3, 7]), su2_rep([1, 1], [2, 4])), [1, 0, 0]),
+    ):
+        ts = SU2SymmetricTensor.random(rows, cols, signature=np.array(sig, dtype=bool), rng=rng)
+        pack_tensor(name + "_su2", ts, data)
+        pack_tensor(name, ts.toO2(), data)
     save("o2", data)
 
 

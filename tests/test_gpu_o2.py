@@ -122,3 +122,15 @@ def test_o2_native_kernels_launched():
     after = _native.CALL_COUNTS
     assert after.get("fs_o2_recombine", 0) - before.get("fs_o2_recombine", 0) == 2
     assert after.get("fs_abelian_permute", 0) - before.get("fs_abelian_permute", 0) == 1
+
+
+@pytest.mark.parametrize("name", ["su2cast_int", "su2cast_half", "su2cast_mixed"])
+def test_su2_to_o2_cast_matches_reference(name):
+    """SU2SymmetricTensor.toO2 (su2_symmetric_tensor.py:249-318)."""
+    from frostspin_b200 import SU2SymmetricTensor
+
+    d = load("o2")
+    ts = SU2SymmetricTensor.load_from_dic(d, prefix=name + "_su2")
+    to2 = ts.cast("O2")
+    check_against(to2, d, name, tol=1e-13)
+    assert abs(to2.norm() - ts.norm()) <= 1e-13 * ts.norm()

@@ -174,3 +174,19 @@ def test_o2_structure_functions():
     r = np.array([[1, 2, 1, 2], [-1, 0, 1, 2]])
     assert np.array_equal(o2m.rep_to_u1(r), [0, 0, 0, 1, -1, 2, 2, -2, -2])
     assert O2SymmetricTensor.representation_dimension(r) == 9
+
+
+def test_su2_to_o2_leg_maps_match_oracle():
+    """Per-leg order, signs and O(2) representation of the SU(2) -> O(2) cast
+    (su2_symmetric_tensor.py:272-304) against the oracle's loop restatement."""
+    from oracle import o2_oracle as oo
+    from frostspin_b200.symmetric_tensor.su2_symmetric_tensor import _o2_leg
+
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        k = int(rng.integers(1, 5))
+        irr = np.sort(rng.choice(np.arange(1, 12), k, replace=False))
+        rep = np.array([rng.integers(1, 4, k), irr])
+        r1, o1, s1 = _o2_leg(rep)
+        r2, o2, s2 = oo.su2_leg_to_o2(rep)
+        assert np.array_equal(r1, r2) and np.array_equal(o1, o2) and np.array_equal(s1, s2)

@@ -95,3 +95,13 @@ def test_o2_oracle_group_data_and_linear_algebra():
     irr, shapes = oo.get_block_sizes(t.row_reps, t.col_reps, t.signature)
     assert np.array_equal(irr, t.block_irreps)
     assert np.array_equal(shapes, [b.shape for b in t.blocks])
+
+
+@pytest.mark.parametrize("name", ["su2cast_int", "su2cast_half", "su2cast_mixed"])
+def test_o2_oracle_su2_cast(name):
+    from oracle import su2_oracle as so
+
+    d = load("o2")
+    ts = from_dic(d, name + "_su2", so)
+    got = oo.from_su2_dense(so.toarray(ts), ts.row_reps, ts.col_reps, ts.signature)
+    check(got, d, name)
