@@ -9,6 +9,9 @@ cg_tensor evaluates every coefficient with sympy's exact CG routine and casts it
 to float64, the same published routine and conversion the reference used to
 write its table, so the values are identical to the reference's (a correctly
 rounded evaluation differs from them by one ulp on about a third of the tensors).
+Tensors with every dimension <= 18 come from su2_cg_table.npz, the same sympy
+values written once by make_su2_cg_table.py, which saves the sympy import and
+evaluation (seconds) on first use; larger ones are evaluated on demand.
 cg_coefficient is an independent evaluation by Racah's closed formula
 (G. Racah, Phys. Rev. 62, 438 (1942)) in exact rational arithmetic, used to
 cross-check.  There is no size limit: tensors are generated when first needed
@@ -16,6 +19,7 @@ and cached.
 """
 
 import decimal
+import os
 from fractions import Fraction
 from functools import lru_cache
 from math import factorial
@@ -23,6 +27,9 @@ from math import factorial
 import numpy as np
 
 _CTX = decimal.Context(prec=60)
+
+TABLE_FILE = "su2_cg_table.npz"
+_PACKED = {}
 
 # coefficients loaded from a table file, (d1, d2, d3) -> (flat indices, values);
 # tensors missing from it are computed
@@ -68,14 +75,34 @@ def cg_coefficient(d1, i1, d2, i2, d3, i3):
     return sq if s > 0 else -sq
 
 
-def _nonzero_entries(d1, d2, d3):
+def nonzero_entries(d1, d2, d3):
+    """(i1, i2, i3) index arrays of the structurally allowed entries (m1 + m2 =
+    m3), in C order of (i1, i2)."""
     j1, j2, j3 = d1 - 1, d2 - 1, d3 - 1
-    for i1 in range(d1):
-        for i2 in range(d2):
-            m3 = (j1 - 2 * i1) + (j2 - 2 * i2)
-            if abs(m3) > j3 or (j3 - m3) % 2:
-                continue
-            yield i1, i2, (j3 - m3) // 2
+    i1, i2 = np.meshgrid(np.arange(d1), np.arange(d2), indexing="ij")
+    m3 = (j1 - 2 * i1) + (j2 - 2 * i2)
+    ok = (np.abs(m3) <= j3) & ((j3 - m3) % 2 == 0)
+    return i1[ok], i2[ok], (j3 - m3[ok]) // 2
+
+
+def _nonzero_entries(d1, d2, d3):
+    yield from zip(*(x.tolist() for x in nonzero_entries(d1, d2, d3)), strict=True)
+
+
+def _packed_table():
+    """Packaged coefficients: (d1, d2, d3) -> values in nonzero_entries order."""
+    if not _PACKED:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), TABLE_FILE)
+        index = {}
+        if os.path.exists(path):
+            with np.load(path) as f:
+                values = f["values"]
+                offsets = f["offsets"]
+                for k, t in enumerate(f["triples"].tolist()):
+                    index[tuple(t)] = (int(offsets[k]), int(offsets[k + 1]))
+            _PACKED["values"] = values
+        _PACKED["index"] = index
+    return _PACKED
 
 
 def set_table(table):
@@ -96,6 +123,18 @@ def cg_tensor(d1, d2, d3):
         p = p.reshape(d1, d2, d3)
         p.setflags(write=False)
         return p
+    packed = _packed_table()
+    span = packed["index"].get((d1, d2, d3))
+    if span is not None:
+        p = np.zeros((d1, d2, d3))
+        p[nonzero_entries(d1, d2, d3)] = packed["values"][span[0] : span[1]]
+        p.setflags(write=False)
+        return p
+    return cg_tensor_sympy(d1, d2, d3)
+
+
+def cg_tensor_sympy(d1, d2, d3):
+    """p[i1, i2, i3] from sympy's exact CG routine, cast to float64."""
     import sympy as sp
     from sympy.physics.quantum.cg import CG
 

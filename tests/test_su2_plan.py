@@ -156,3 +156,18 @@ def test_cg_coefficients_against_closed_form():
                 a = su2_cg.cg_tensor(d1, d2, d3)
                 b = su2_cg.cg_tensor_racah(d1, d2, d3)
                 assert np.abs(a - b).max() <= 2.3e-16
+
+
+def test_packaged_cg_table_equals_sympy_evaluation():
+    """The packaged table holds sympy's float64 values bit for bit (sampled,
+    the largest tensors included), and covers every dimension up to 18."""
+    rng = np.random.default_rng(2)
+    packed = su2_cg._packed_table()["index"]
+    assert (18, 18, 35 - 18) in packed and (17, 5, 13) in packed
+    triples = sorted(packed)
+    picks = [triples[i] for i in rng.choice(len(triples), 12, replace=False)]
+    picks += [(18, 17, 18), (9, 9, 17), (17, 5, 13), (1, 1, 1)]
+    for d1, d2, d3 in picks:
+        a = su2_cg.cg_tensor(d1, d2, d3)
+        b = su2_cg.cg_tensor_sympy(d1, d2, d3)
+        assert np.array_equal(a, b), (d1, d2, d3)
