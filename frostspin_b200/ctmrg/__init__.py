@@ -8,10 +8,12 @@ from .classical_c4v import (
 )
 from .ctm_environment import CTMEnvironment
 from .sequential_ctmrg import SequentialCTMRG
+from .simultaneous_ctmrg import SimultaneousCTMRG
 
 __all__ = [
     "CTMEnvironment",
     "SequentialCTMRG",
+    "SimultaneousCTMRG",
     "energy_per_bond",
     "env_1site",
     "env_2sites",

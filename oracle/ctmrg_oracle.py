@@ -353,3 +353,62 @@ def ctm_rdm2x1(ctm, x, y):
         g("T4", x, y + 1).permute((1, 2, 3), (0,)), g("T4", x, y + 2).permute((1, 2, 3), (0,)),
         g("C4", x, y + 3).transpose(),
     )
+
+
+def ren_quadrant(P, quadrant, Pt):
+    """ctm_renormalize.py:219-225."""
+    return (P.transpose() @ quadrant @ Pt).normalized()
+
+
+class SimultaneousCTMRG(SequentialCTMRG):
+    """simultaneous_ctmrg.py:14-132 with the checkerboard AB/BA cell: every
+    enlarged corner, then the projectors of the four directions, then every
+    corner (from the enlarged corners) and edge of every site at once."""
+
+    def iterate(self):
+        g, A = self.g, self.A
+        idx = self.idx
+        for x, y in self.coords:
+            for kind in ("dr", "ur", "ul", "dl"):
+                self.corner(kind, x, y)
+        pr = {d: {} for d in ("up", "right", "down", "left")}
+        for x, y in self.coords:
+            dl, dr, ur, ul = (self.corner(k, x, y) for k in ("dl", "dr", "ur", "ul"))
+            pr["up"][idx(x + 2, y)] = self._proj(dr, ur, ul, dl)
+            pr["right"][idx(x + 3, y + 2)] = self._proj(dl, dr, ur, ul)
+            pr["down"][idx(x + 1, y + 3)] = self._proj(ul, dl, dr, ur)
+            pr["left"][idx(x, y + 1)] = self._proj(ur, ul, dl, dr)
+
+        def P(d, x, y):
+            return pr[d][idx(x, y)][0]
+
+        def Pt(d, x, y):
+            return pr[d][idx(x, y)][1]
+
+        names = ("C1", "C2", "C3", "C4", "T1", "T2", "T3", "T4")
+        new = {k: [None, None] for k in names}
+        for x, y in self.coords:
+            i = idx(x, y)
+            a = A(x, y)
+            new["C1"][i] = ren_quadrant(P("up", x + 1, y - 1), self.corner("ul", x - 1, y - 1),
+                                        Pt("left", x - 1, y))
+            new["T1"][i] = ren_T(Pt("up", x, y - 1), g("T1", x, y - 1).permute((1, 2, 3), (0,)),
+                                 a.permute((0, 1, 4, 5), (2, 3)),
+                                 P("up", x + 1, y - 1)).permute((3,), (1, 2, 0))
+            new["C2"][i] = ren_quadrant(P("right", x + 1, y + 1), self.corner("ur", x - 2, y - 1),
+                                        Pt("up", x, y - 1))
+            new["T2"][i] = ren_T(Pt("right", x + 1, y), g("T2", x + 1, y).permute((2, 3, 0), (1,)),
+                                 a.permute((0, 1, 5, 2), (3, 4)),
+                                 P("right", x + 1, y + 1)).permute((0,), (3, 1, 2))
+            new["C3"][i] = ren_quadrant(P("down", x - 1, y + 1), self.corner("dr", x - 2, y - 2),
+                                        Pt("right", x + 1, y)).transpose()
+            new["T3"][i] = ren_T(Pt("down", x, y + 1), g("T3", x, y + 1).permute((0, 1, 2), (3,)),
+                                 a.permute((0, 1, 2, 3), (4, 5)),
+                                 P("down", x - 1, y + 1)).permute((1, 2, 0), (3,))
+            new["C4"][i] = ren_quadrant(P("left", x - 1, y - 1), self.corner("dl", x - 1, y - 2),
+                                        Pt("down", x, y + 1))
+            new["T4"][i] = ren_T(Pt("left", x - 1, y), g("T4", x - 1, y).permute((1, 2, 3), (0,)),
+                                 a.permute((0, 1, 3, 4), (5, 2)),
+                                 P("left", x - 1, y - 1)).permute((3,), (1, 2, 0))
+        self.t = new
+        self.corners = {k: [None, None] for k in ("ul", "ur", "dl", "dr")}

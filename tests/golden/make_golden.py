@@ -386,6 +386,31 @@ def case_simple_update_su2():
     save("simple_update_su2", data)
 
 
+def case_simultaneous_ctmrg():
+    """SimultaneousCTMRG (simultaneous_ctmrg.py:14-132) of the reference on
+    two existing fixtures' site tensors: the random U(1) AB/BA network and the
+    SU(2) simple-update tensors; chi = 20, 3 iterations; chi values, rdms and
+    the PEPS norm after each."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.ctmrg import SimultaneousCTMRG
+
+    data = {}
+    for tag, cls, fix, names in (("u1", U1SymmetricTensor, "ctmrg_u1_random", ("A", "B")),
+                                 ("su2", SU2SymmetricTensor, "simple_update_su2", ("A0", "A1"))):
+        d = np.load(os.path.join(HERE, fix + ".npz"))
+        tensors = [cls.load_from_dic(d, prefix=p) for p in names]
+        ctm = SimultaneousCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                        degen_ratio=0.9999)
+        for it in range(3):
+            ctm.iterate()
+            data[f"{tag}_it{it}_chi"] = np.array(ctm.chi_values)
+            for (x, y) in ctm.site_coords:
+                data[f"{tag}_it{it}_rdm1x2_{x}{y}"] = ctm.compute_rdm1x2(x, y).toarray()
+                data[f"{tag}_it{it}_rdm2x1_{x}{y}"] = ctm.compute_rdm2x1(x, y).toarray()
+            data[f"{tag}_it{it}_logZ"] = np.array(ctm.compute_PEPS_norm_log())
+    save("simultaneous_ctmrg", data)
+
+
 def case_su2_d24_beta2():
     """Site tensors of the SU(2) CTMRG benchmark: the reference's SU(2) simple
     update of the Heisenberg model, D=24, tau=0.01, evolved to beta=2."""

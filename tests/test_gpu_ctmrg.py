@@ -98,3 +98,32 @@ def test_su2_ctmrg_from_reference_d24_tensors():
         assert np.abs(r21 - ref[f"rdm2x1_{x}{y}"]).max() < 1e-9
         es += [np.einsum("ijkl,klij->", r12, sds), np.einsum("ijkl,klij->", r21, sds)]
     assert abs(np.mean(es) - float(ref["energy"])) < 1e-10
+
+
+@pytest.mark.parametrize("tag", ["u1", "su2"])
+def test_simultaneous_ctmrg_matches_reference(tag):
+    """SimultaneousCTMRG (simultaneous_ctmrg.py:14-132) against the reference's
+    run on the same tensors: chi values, rdms and the PEPS norm after each of 3
+    iterations at chi = 20."""
+    from frostspin_b200 import SU2SymmetricTensor, U1SymmetricTensor
+    from frostspin_b200.ctmrg import SimultaneousCTMRG
+
+    ref = load("simultaneous_ctmrg")
+    if tag == "su2":
+        d = load("simple_update_su2")
+        tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
+    else:
+        d = load("ctmrg_u1_random")
+        tensors = [U1SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A", "B")]
+    ctm = SimultaneousCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    assert "SimultaneousCTMRG" in repr(ctm)
+    for it in range(3):
+        ctm.iterate()
+        assert ctm.chi_values == list(ref[f"{tag}_it{it}_chi"]), it
+        for x, y in ctm.site_coords:
+            for kind, fn in (("rdm1x2", ctm.compute_rdm1x2), ("rdm2x1", ctm.compute_rdm2x1)):
+                r = ref[f"{tag}_it{it}_{kind}_{x}{y}"]
+                got = fn(x, y).toarray()
+                assert np.abs(got - r).max() < 1e-8 * max(1.0, np.abs(r).max()), (it, kind)
+        assert abs(ctm.compute_PEPS_norm_log() - float(ref[f"{tag}_it{it}_logZ"])) < 1e-8
