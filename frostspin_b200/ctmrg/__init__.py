@@ -9,11 +9,13 @@ from .classical_c4v import (
 from .ctm_environment import CTMEnvironment
 from .sequential_ctmrg import SequentialCTMRG
 from .simultaneous_ctmrg import SimultaneousCTMRG
+from .symmetrized_ctmrg import SymmetrizedCTMRG
 
 __all__ = [
     "CTMEnvironment",
     "SequentialCTMRG",
     "SimultaneousCTMRG",
+    "SymmetrizedCTMRG",
     "energy_per_bond",
     "env_1site",
     "env_2sites",

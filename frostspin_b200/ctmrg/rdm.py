@@ -77,3 +77,69 @@ def rdm_2x1(C1, T1, C2, T4u, Au, T2u, T4d, Ad, T2d, C4, T3, C3):
         T4d.permute((1, 2, 3), (0,)),
         C4.transpose(),
     )
+
+
+def rdm_symmetrized_1x2(C1, T1l, T4, Al, C4, T3l):
+    """Two sites in a row when the right half is the mirror image of the left
+    one (environment of SymmetrizedCTMRG, B = rotated dagger of A;
+    rdm.py:139-153): the left half is contracted once and reused, permuted."""
+    left = T4.permute((0, 1, 2), (3,)) @ C4
+    left = contract_open_corner(C1, T1l, left, Al)
+    left = left @ T3l.permute((0, 1, 3), (2,))
+    left = left.permute((0, 1), (2, 3, 4, 5))
+    right = left.permute((3, 2, 5, 4), (1, 0))
+    r = (left @ right).permute((1, 3), (0, 2))
+    r /= r.trace()
+    return r
+
+
+def rdm_symmetrized_2x1(C1, T1, C2, T4u, Au, T2u):
+    """Two sites in a column, symmetrized environment (rdm.py:156-168)."""
+    return rdm_symmetrized_1x2(
+        C2,
+        T2u.permute((1, 2, 3), (0,)),
+        T1,
+        Au.permute((0, 1), (3, 4, 5, 2)),
+        C1,
+        T4u.permute((1, 2, 3), (0,)),
+    )
+
+
+def rdm_diag_dr(C1, T1l, ur, T4u, Aul, dl, Adr, T2d, T3r, C3):
+    """Second neighbours on the down-right diagonal of a 2x2 plaquette
+    (rdm.py:190-238): the open upper-left corner, closed with the enlarged
+    down-left and upper-right corners, then the open down-right corner."""
+    r = contract_open_corner(C1, T1l, T4u, Aul)
+    r = r @ dl
+    r = r.permute((2, 3, 4), (0, 1, 5, 6, 7))
+    r = ur @ r
+    r = r.permute((3, 4), (0, 1, 2, 5, 6, 7))
+    dr = contract_open_corner_mirror(
+        T2d.permute((1, 2, 3), (0,)),
+        C3.transpose(),
+        Adr.permute((0, 1, 3, 4), (5, 2)),
+        T3r.permute((2, 3), (0, 1)),
+    )
+    dr = dr.permute((5, 2, 6, 4, 1, 7), (3, 0))
+    r = (r @ dr).permute((1, 3), (0, 2))
+    r /= r.trace()
+    return r
+
+
+def rdm_diag_ur(ul, T1r, C2, Aur, T2u, T4d, Adl, dr_T, C4, T3l):
+    """Second neighbours on the up-right diagonal (rdm.py:241-269), through
+    rdm_diag_dr on the plaquette rotated by a quarter turn; dr_T is the
+    enlarged down-right corner in transposed leg order."""
+    r = rdm_diag_dr(
+        C4,
+        T4d,
+        ul,
+        T3l.permute((3,), (0, 1, 2)),
+        Adl.permute((0, 1), (5, 2, 3, 4)),
+        dr_T,
+        Aur.permute((0, 1), (5, 2, 3, 4)),
+        T1r.permute((3,), (0, 1, 2)),
+        T2u.permute((2, 3, 0), (1,)),
+        C2.transpose(),
+    )
+    return r.permute((1, 0), (3, 2))

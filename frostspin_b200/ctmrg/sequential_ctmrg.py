@@ -357,3 +357,42 @@ class SequentialCTMRG:
         r12 = [self.compute_rdm1x2(x, y) for x, y in self.site_coords]
         r21 = [self.compute_rdm2x1(x, y) for x, y in self.site_coords]
         return r12, r21
+
+    def compute_rdm1x1_cell(self):
+        """abstract_ctmrg.py:476-483."""
+        return [self.compute_rdm1x1(x, y) for x, y in self.site_coords]
+
+    def compute_rdm_diag_dr(self, x, y, *, free_memory=False):
+        """abstract_ctmrg.py:438-455: sites (x + 1, y + 1) and (x + 2, y + 2)."""
+        e = self._env
+        return rdm.rdm_diag_dr(
+            e.get_C1(x, y), e.get_T1(x + 1, y),
+            self.construct_enlarged_ur(x, y, free_memory=free_memory),
+            e.get_T4(x, y + 1), e.get_A(x + 1, y + 1),
+            self.construct_enlarged_dl(x, y, free_memory=free_memory),
+            e.get_A(x + 2, y + 2), e.get_T2(x + 3, y + 2), e.get_T3(x + 2, y + 3),
+            e.get_C3(x + 3, y + 3),
+        )
+
+    def compute_rdm_diag_ur(self, x, y, *, free_memory=False):
+        """abstract_ctmrg.py:457-474: sites (x + 1, y + 2) and (x + 2, y + 1)."""
+        e = self._env
+        return rdm.rdm_diag_ur(
+            self.construct_enlarged_ul(x, y, free_memory=free_memory),
+            e.get_T1(x + 2, y), e.get_C2(x + 3, y), e.get_A(x + 2, y + 1),
+            e.get_T2(x + 3, y + 1), e.get_T4(x, y + 2), e.get_A(x + 1, y + 2),
+            self.construct_enlarged_dr(x, y, free_memory=free_memory),
+            e.get_C4(x, y + 3), e.get_T3(x + 1, y + 3),
+        )
+
+    def compute_rdm_2nd_neighbor_cell(self, *, free_memory=True):
+        """abstract_ctmrg.py:501-517: both diagonals of every unique site.  With
+        free_memory the cached enlarged corners are dropped first and each is
+        freed after use (the contraction peaks at 3 d^2 chi^2 D^4)."""
+        if free_memory:
+            self._env.reset_constructed_corners()
+        dr, ur = [], []
+        for x, y in self.site_coords:
+            dr.append(self.compute_rdm_diag_dr(x, y, free_memory=free_memory))
+            ur.append(self.compute_rdm_diag_ur(x, y, free_memory=free_memory))
+        return dr, ur

@@ -411,6 +411,55 @@ def case_simultaneous_ctmrg():
     save("simultaneous_ctmrg", data)
 
 
+def case_ctmrg_variants():
+    """Second-neighbour observables (abstract_ctmrg.py:438-518, rdm.py:190-269)
+    of the reference's SequentialCTMRG on the SU(2) simple-update tensors, and
+    SymmetrizedCTMRG (symmetrized_ctmrg.py:19-274) on the input of the
+    reference's tests/test_symmetrized_ctm.py (random SU(2) site tensor, seed
+    42, B = rotated dagger of A, chi = 50): chi values, rdms and PEPS norm
+    after each of 3 iterations, then the second-neighbour rdms."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.ctmrg import SequentialCTMRG, SymmetrizedCTMRG
+
+    data = {}
+    d = np.load(os.path.join(HERE, "simple_update_su2.npz"))
+    tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for _ in range(3):
+        ctm.iterate()
+    for i, r in enumerate(ctm.compute_rdm1x1_cell()):
+        data[f"seq_rdm1x1_{i}"] = r.toarray()
+    dr, ur = ctm.compute_rdm_2nd_neighbor_cell()
+    for i, (a, b) in enumerate(zip(dr, ur, strict=True)):
+        data[f"seq_rdm_dr_{i}"] = a.toarray()
+        data[f"seq_rdm_ur_{i}"] = b.toarray()
+
+    rng = np.random.default_rng(42)
+    r2 = np.array([[1], [2]])
+    rDu = np.array([[2, 3], [1, 3]])
+    rDr = np.array([[3, 3], [1, 3]])
+    rDd = np.array([[1, 3], [1, 3]])
+    rDl = np.array([[4, 3], [1, 3]])
+    A = SU2SymmetricTensor.random((r2, r2), (rDu, rDr, rDd, rDl), rng=rng)
+    A /= A.norm()
+    pack_tensor("symA", A, data)
+    B = A.dagger().permute((4, 5), (2, 3, 0, 1))
+    ctm = SymmetrizedCTMRG.from_elementary_tensors("AB\nBA", [A, B], 50)
+    data["sym_it-1_logZ"] = np.array(ctm.compute_PEPS_norm_log())
+    for it in range(3):
+        ctm.iterate()
+        data[f"sym_it{it}_chi"] = np.array(ctm.chi_values)
+        for (x, y) in ctm.site_coords:
+            data[f"sym_it{it}_rdm1x2_{x}{y}"] = ctm.compute_rdm1x2(x, y).toarray()
+            data[f"sym_it{it}_rdm2x1_{x}{y}"] = ctm.compute_rdm2x1(x, y).toarray()
+        data[f"sym_it{it}_logZ"] = np.array(ctm.compute_PEPS_norm_log())
+    (dr0, dr1), (ur0, ur1) = ctm.compute_rdm_2nd_neighbor_cell()
+    data["sym_rdm_dr"] = dr0.toarray()
+    data["sym_rdm_ur"] = ur0.toarray()
+    save("ctmrg_variants", data)
+
+
 def case_su2_d24_beta2():
     """Site tensors of the SU(2) CTMRG benchmark: the reference's SU(2) simple
     update of the Heisenberg model, D=24, tau=0.01, evolved to beta=2."""

@@ -127,3 +127,52 @@ def test_simultaneous_ctmrg_matches_reference(tag):
                 got = fn(x, y).toarray()
                 assert np.abs(got - r).max() < 1e-8 * max(1.0, np.abs(r).max()), (it, kind)
         assert abs(ctm.compute_PEPS_norm_log() - float(ref[f"{tag}_it{it}_logZ"])) < 1e-8
+
+
+def test_second_neighbor_rdms_match_reference():
+    """compute_rdm1x1_cell and compute_rdm_2nd_neighbor_cell
+    (abstract_ctmrg.py:438-518, rdm.py:190-269) after 3 SequentialCTMRG
+    iterations at chi = 20 on the SU(2) simple-update tensors."""
+    from frostspin_b200 import SU2SymmetricTensor
+    from frostspin_b200.ctmrg import SequentialCTMRG
+
+    ref = load("ctmrg_variants")
+    d = load("simple_update_su2")
+    tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for _ in range(3):
+        ctm.iterate()
+    for i, r in enumerate(ctm.compute_rdm1x1_cell()):
+        assert np.abs(r.toarray() - ref[f"seq_rdm1x1_{i}"]).max() < 1e-8
+    dr, ur = ctm.compute_rdm_2nd_neighbor_cell()
+    for i, (a, b) in enumerate(zip(dr, ur, strict=True)):
+        assert np.abs(a.toarray() - ref[f"seq_rdm_dr_{i}"]).max() < 1e-8
+        assert np.abs(b.toarray() - ref[f"seq_rdm_ur_{i}"]).max() < 1e-8
+
+
+def test_symmetrized_ctmrg_matches_reference():
+    """SymmetrizedCTMRG (symmetrized_ctmrg.py:19-274) on the input of the
+    reference's tests/test_symmetrized_ctm.py (B = rotated dagger of A,
+    chi = 50): PEPS norm before and after each of 3 iterations, chi values,
+    nearest- and second-neighbour rdms."""
+    from frostspin_b200 import SU2SymmetricTensor
+    from frostspin_b200.ctmrg import SymmetrizedCTMRG
+
+    ref = load("ctmrg_variants")
+    A = SU2SymmetricTensor.load_from_dic(ref, prefix="symA")
+    B = A.dagger().permute((4, 5), (2, 3, 0, 1))
+    ctm = SymmetrizedCTMRG.from_elementary_tensors("AB\nBA", [A, B], 50)
+    assert "SymmetrizedCTMRG" in repr(ctm)
+    assert abs(ctm.compute_PEPS_norm_log() - float(ref["sym_it-1_logZ"])) < 1e-10
+    for it in range(3):
+        ctm.iterate()
+        assert ctm.chi_values == list(ref[f"sym_it{it}_chi"]), it
+        for x, y in ctm.site_coords:
+            for kind, fn in (("rdm1x2", ctm.compute_rdm1x2), ("rdm2x1", ctm.compute_rdm2x1)):
+                r = ref[f"sym_it{it}_{kind}_{x}{y}"]
+                assert np.abs(fn(x, y).toarray() - r).max() < 1e-8, (it, kind)
+        assert abs(ctm.compute_PEPS_norm_log() - float(ref[f"sym_it{it}_logZ"])) < 1e-8
+    (dr, _), (ur, _) = ctm.compute_rdm_2nd_neighbor_cell()
+    assert np.abs(dr.toarray() - ref["sym_rdm_dr"]).max() < 1e-8
+    assert np.abs(ur.toarray() - ref["sym_rdm_ur"]).max() < 1e-8

@@ -43,3 +43,29 @@ def test_simultaneous_ctmrg_oracle_matches_reference_run(tag):
             for kind, fn in (("rdm1x2", co.ctm_rdm1x2), ("rdm2x1", co.ctm_rdm2x1)):
                 r = ref[f"{tag}_it{it}_{kind}_{x}{y}"]
                 assert np.abs(fn(ctm, x, y) - r).max() < 1e-8 * max(1.0, np.abs(r).max())
+
+
+def test_symmetrized_reference_run_equals_simultaneous_oracle():
+    """With B the rotated dagger of A the symmetrized and simultaneous
+    algorithms build the same environment: the oracle's SimultaneousCTMRG on
+    the input of the reference's tests/test_symmetrized_ctm.py reproduces the
+    reference's SymmetrizedCTMRG chi values and rdms (tests/golden/
+    ctmrg_variants.npz), which pins that fixture independently."""
+    ref = load("ctmrg_variants")
+    p = "symA"
+    nrr = int(ref[p + "_n_row_reps"])
+    ncr = int(ref[p + "_n_col_reps"])
+    irr = ref[p + "_block_irreps"]
+    A = so.OTensor([ref[f"{p}_row_rep_{i}"] for i in range(nrr)],
+                   [ref[f"{p}_col_rep_{i}"] for i in range(ncr)],
+                   [ref[f"{p}_block_{i}"] for i in range(irr.size)], irr, ref[p + "_signature"])
+    B = so.permute(so.dagger(A), (4, 5), (2, 3, 0, 1))
+    ctm = co.SimultaneousCTMRG(A, B, 50, cutoff=1e-11, degen_ratio=0.9999)
+    for it in range(3):
+        ctm.iterate()
+        chi = sorted({s for C in ctm.t["C1"] + ctm.t["C3"] for s in C.shape})
+        assert chi == list(ref[f"sym_it{it}_chi"]), it
+        for x, y in ctm.coords:
+            for kind, fn in (("rdm1x2", co.ctm_rdm1x2), ("rdm2x1", co.ctm_rdm2x1)):
+                r = ref[f"sym_it{it}_{kind}_{x}{y}"]
+                assert np.abs(fn(ctm, x, y) - r).max() < 1e-12
