@@ -190,3 +190,63 @@ def test_su2_to_o2_leg_maps_match_oracle():
         r1, o1, s1 = _o2_leg(rep)
         r2, o2, s2 = oo.su2_leg_to_o2(rep)
         assert np.array_equal(r1, r2) and np.array_equal(o1, o2) and np.array_equal(s1, s2)
+
+
+def _random_o2_rep(rng):
+    irreps = [q for q in (-1, 0) if rng.random() < 0.6]
+    irreps += sorted(rng.choice(np.arange(1, 4), int(rng.integers(1, 3)), replace=False).tolist())
+    return np.array([rng.integers(1, 3, len(irreps)), irreps])
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_o2_permute_pipeline_random_against_oracle(seed):
+    """Random O(2) tensors (with or without 0odd / 0even on each leg, any
+    signature, plain or transposed storage), random permutations: the
+    emulated device pipeline equals the oracle's permute, itself pinned to the
+    reference's outputs."""
+    from oracle import o2_oracle as oo
+
+    rng = np.random.default_rng(100 + seed)
+    ndim = int(rng.integers(3, 6))
+    nrr = int(rng.integers(1, ndim))
+    reps = [_random_o2_rep(rng) for _ in range(ndim)]
+    sig = rng.random(ndim) < 0.5
+    ot = oo.random(reps[:nrr], reps[nrr:], sig, rng=rng)
+    if ot.block_irreps.size == 0:
+        return
+    trans = bool(seed % 2)
+    flat = np.concatenate([(b.T if trans else b).ravel() for b in ot.blocks])
+    shapes = np.array([b.shape for b in ot.blocks], dtype=np.int64)
+    offsets = np.concatenate(([0], np.cumsum(shapes[:, 0] * shapes[:, 1])[:-1]))
+    t = O2SymmetricTensor._from_storage(reps[:nrr], reps[nrr:], torch.from_numpy(flat), offsets,
+                                        shapes, ot.block_irreps, sig, trans)
+    p_to = o2m._to_u1_plan(t)
+    u1_flat = emulate_recombine(p_to, flat)
+    tu1 = U1SymmetricTensor._from_storage(
+        [o2m.rep_to_u1(r) for r in reps[:nrr]], [o2m.rep_to_u1(r) for r in reps[nrr:]],
+        torch.from_numpy(u1_flat), p_to.offsets, p_to.shapes,
+        np.asarray(p_to.irreps, dtype=np.int8), sig)
+    for _ in range(3):
+        axes = tuple(int(a) for a in rng.permutation(ndim))
+        new_nrr = int(rng.integers(1, ndim))
+        aplan = tu1._permute_plan(axes, new_nrr)
+        pflat = emulate_permute(aplan, u1_flat)
+        u1reps = tu1.row_reps + tu1.col_reps
+        pu1 = U1SymmetricTensor._from_storage(
+            [u1reps[a] for a in axes[:new_nrr]], [u1reps[a] for a in axes[new_nrr:]],
+            torch.from_numpy(pflat), aplan.offsets, aplan.block_shapes, aplan.block_irreps,
+            sig[list(axes)])
+        back = o2m._from_u1_plan(pu1, [reps[a] for a in axes[:new_nrr]],
+                                 [reps[a] for a in axes[new_nrr:]])
+        got = blocks_of(emulate_recombine(back, pflat), back.offsets, back.shapes)
+        ref = oo.permute(ot, axes[:new_nrr], axes[new_nrr:])
+        assert np.array_equal(np.asarray(back.irreps), ref.block_irreps)
+        for g, b in zip(got, ref.blocks, strict=True):
+            assert g.shape == b.shape
+            assert np.abs(g - b).max(initial=0.0) <= 1e-14 * max(1.0, np.abs(b).max())
+    # the transpose map too
+    tp = o2m._transpose_plan(t)
+    got = blocks_of(emulate_recombine(tp, flat), tp.offsets, tp.shapes[:, ::-1], trans=True)
+    ref = oo.transpose(ot)
+    for g, b in zip(got, ref.blocks, strict=True):
+        assert np.abs(g - b).max(initial=0.0) <= 1e-14 * max(1.0, np.abs(b).max())
