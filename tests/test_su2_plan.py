@@ -171,3 +171,42 @@ def test_packaged_cg_table_equals_sympy_evaluation():
         a = su2_cg.cg_tensor(d1, d2, d3)
         b = su2_cg.cg_tensor_sympy(d1, d2, d3)
         assert np.array_equal(a, b), (d1, d2, d3)
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_su2_permute_tables_random_against_oracle(seed):
+    """Random SU(2) tensors (several irreps and degeneracies per leg, any
+    signature, plain or transposed storage) and random permutations: the
+    gather -> recoupling GEMM -> scatter tables, applied by emulation, equal
+    the oracle's permute, itself pinned to the reference's outputs."""
+    from oracle import su2_oracle as so
+
+    rng = np.random.default_rng(200 + seed)
+    ndim = int(rng.integers(3, 6))
+    nrr = int(rng.integers(1, ndim))
+    reps = []
+    for _ in range(ndim):
+        k = int(rng.integers(1, 3))
+        irr = np.sort(rng.choice(np.arange(1, 5), k, replace=False))
+        reps.append(np.array([rng.integers(1, 3, k), irr]))
+    sig = rng.random(ndim) < 0.5
+    ot = so.random(reps[:nrr], reps[nrr:], sig, rng=rng)
+    if len(ot.blocks) == 0:
+        return
+    trans = bool(seed % 2)
+    flat = np.concatenate([(b.T if trans else b).ravel() for b in ot.blocks])
+    shapes = np.array([b.shape for b in ot.blocks], dtype=np.int64)
+    offsets = np.concatenate(([0], np.cumsum(shapes[:, 0] * shapes[:, 1])[:-1]))
+    t = SU2SymmetricTensor._from_storage(reps[:nrr], reps[nrr:], torch.from_numpy(flat),
+                                         offsets, shapes, ot.block_irreps, sig, trans)
+    for _ in range(2):
+        axes = tuple(int(a) for a in rng.permutation(ndim))
+        new_nrr = int(rng.integers(1, ndim))
+        m = t._permute_map(axes, new_nrr)
+        out = emulate_map(m, flat)
+        ref = so.permute(ot, axes[:new_nrr], axes[new_nrr:])
+        assert np.array_equal(m.out_irreps, ref.block_irreps)
+        scale = max([np.abs(b).max() for b in ref.blocks] + [1e-300])
+        for o, (r, c), b in zip(m.out_offsets, m.out_shapes, ref.blocks, strict=True):
+            assert (r, c) == b.shape
+            assert np.abs(out[o : o + r * c].reshape(r, c) - b).max() <= TOL * scale
