@@ -218,9 +218,11 @@ class _Recombine:
             raise ValueError("O(2) table row index outside its source block")
         if cidx.size and (cidx.min() < 0 or cidx.max() >= n):
             raise ValueError("O(2) table column index outside its source block")
+        if ridx.shape != rcoef.shape or cidx.shape != ccoef.shape:
+            raise ValueError("O(2) table index and coefficient lengths differ")
         rs, cs = self.strides(shape, trans)
         return (int(src_off), rs, cs, self._push(ridx, "i"), self._push(cidx, "i"),
-                self._push(rcoef, "c"), self._push(ccoef, "c"), m * n)
+                self._push(rcoef, "c"), self._push(ccoef, "c"), m * n, ridx.size, cidx.size)
 
     def identity(self, src_off, shape, trans):
         m, n = int(shape[0]), int(shape[1])
@@ -236,7 +238,10 @@ class _Recombine:
         rec["nrows"] = nrows
         rec["ncols"] = ncols
         rec["nterms"] = len(terms)
-        for t, (src_off, rs, cs, ri, ci, rc, cc, _) in enumerate(terms):
+        for t, (src_off, rs, cs, ri, ci, rc, cc, _, nr, nc) in enumerate(terms):
+            # the kernel reads nrows row entries and ncols column entries
+            if (nr, nc) != (nrows, ncols):
+                raise ValueError("O(2) table lengths do not match the output block")
             rec["terms"][t] = (src_off, rs, cs, ri, ci, rc, cc)
         self._blocks.append(rec)
         self._all_terms.append(terms)
@@ -250,7 +255,7 @@ class _Recombine:
         """Freeze the tables; every source term must lie inside the source
         buffer of length src_len."""
         for terms in self._all_terms:
-            for src_off, _, _, _, _, _, _, size in terms:
+            for src_off, _, _, _, _, _, _, size, _, _ in terms:
                 if src_off < 0 or src_off + size > src_len:
                     raise ValueError("O(2) table source block outside the source buffer")
         self.blocks = (np.array(self._blocks, dtype=_native.O2_BLOCK_DTYPE)
