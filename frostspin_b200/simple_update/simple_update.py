@@ -13,6 +13,7 @@ import numpy as np
 
 from ..symmetric_tensor import DiagonalTensor
 from ..symmetric_tensor.tools import get_symmetric_tensor_type
+from .su_models import TENSOR_BOND_INDICES, j1_j2_models
 
 
 def check_tensor_bond_indices(tensor_bond_indices):
@@ -185,6 +186,19 @@ class SimpleUpdate:
         return cls.from_infinite_temperature(D, tau, rcutoff, degen_ratio,
                                              tensor_bond_indices, update_data, [h1],
                                              verbosity=verbosity)
+
+    @classmethod
+    def square_lattice_second_neighbor(cls, h1, h2, D, tau, *, model="J1-J2", rcutoff=1e-10,
+                                       degen_ratio=1.0, verbosity=0):
+        """simple_update.py:366-407: AB//CD plaquette, 8 bonds, first-neighbour
+        gates h1 and second-neighbour gates h2 / 2 applied through both
+        intermediate sites; ``model`` is "J1-J2", "checkerboard" or
+        "Shastry-Sutherland" (su_models.py)."""
+        if model not in j1_j2_models:
+            raise KeyError(f"Unknown model: {model}")
+        return cls.from_infinite_temperature(D, tau, rcutoff, degen_ratio,
+                                             TENSOR_BOND_INDICES, j1_j2_models[model],
+                                             [h1, h2 / 2], verbosity=verbosity)
 
     @classmethod
     def from_infinite_temperature(cls, D, tau, rcutoff, degen_ratio, tensor_bond_indices,

@@ -11,6 +11,7 @@ this script.  The fixtures are what pins the CPU oracle (oracle/) and, through
 it and directly, the device path.  Nothing at test time reads the reference.
 """
 
+import json
 import os
 import sys
 
@@ -458,6 +459,39 @@ def case_ctmrg_variants():
     data["sym_rdm_dr"] = dr0.toarray()
     data["sym_rdm_ur"] = ur0.toarray()
     save("ctmrg_variants", data)
+
+
+def _plain(v):
+    """Nested lists / tuples of numpy scalars -> JSON-able Python values."""
+    if isinstance(v, (list, tuple)):
+        return [_plain(x) for x in v]
+    if v is None:
+        return None
+    return v.item() if hasattr(v, "item") else v
+
+
+def case_su_schedules():
+    """Update schedules of the reference's simple update (get_update_data,
+    simple_update.py:68-184) for the first-neighbour square lattice and the
+    three second-neighbour models of su_models.py, with scalar stand-ins for
+    the Hamiltonians (the schedule only multiplies them by 2)."""
+    from frostspin.simple_update.simple_update import get_update_data
+    from frostspin.simple_update.su_models import j1_j2_models
+
+    data = {}
+    cases = {"first": ([[0, 1, 2, 3], [2, 3, 0, 1]],
+                       np.array([[b, b, 0, 0, 1, -1] for b in range(4)]), [1.0])}
+    tbi2 = [[0, 1, 2, 3], [4, 3, 5, 1], [2, 6, 0, 7], [5, 7, 4, 6]]
+    for name, table in j1_j2_models.items():
+        cases[name] = (tbi2, table, [1.0, 0.5])
+    for name, (tbi, table, hams) in cases.items():
+        out = get_update_data(tbi, table, hams)
+        keys = ("bond1", "bond2", "gate", "left", "right", "middle", "lperm", "rperm",
+                "mperm", "hamiltonians", "initial_swap", "final_swap")
+        for k, v in zip(keys, out, strict=True):
+            data[f"{name}_{k}"] = np.array(json.dumps(_plain(v)))
+        data[f"{name}_table"] = np.asarray(table)
+    save("su_schedules", data)
 
 
 def case_su2_d24_beta2():
