@@ -494,6 +494,30 @@ def case_su_schedules():
     save("su_schedules", data)
 
 
+def case_simple_update_j1j2():
+    """U(1) J1-J2 simple update of the reference (square_lattice_second_neighbor,
+    simple_update.py:366-407; J2 = 0.5, D = 4, tau = 0.01) for each model, two
+    evolve steps: weights, logZ and bond representations."""
+    from frostspin.simple_update import SimpleUpdate
+
+    reps = (np.array([1, -1], dtype=np.int8),) * 2
+    h1 = U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
+    data = {}
+    pack_tensor("h1", h1, data)
+    for model in ("J1-J2", "checkerboard", "Shastry-Sutherland"):
+        su = SimpleUpdate.square_lattice_second_neighbor(h1, 0.5 * h1, 4, 0.01, model=model,
+                                                         rcutoff=1e-10, degen_ratio=0.9999)
+        for k in range(2):
+            su.evolve(0.04)
+            data[f"{model}_b{k}_beta"] = np.array(su.beta)
+            data[f"{model}_b{k}_logZ"] = np.array(su.logZ)
+            for i, w in enumerate(su.get_weights()):
+                data[f"{model}_b{k}_w{i}"] = w
+            for i, r in enumerate(su.get_bond_representations()):
+                data[f"{model}_b{k}_rep{i}"] = r
+    save("simple_update_j1j2", data)
+
+
 def case_su2_d24_beta2():
     """Site tensors of the SU(2) CTMRG benchmark: the reference's SU(2) simple
     update of the Heisenberg model, D=24, tau=0.01, evolved to beta=2."""

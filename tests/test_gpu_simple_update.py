@@ -95,3 +95,27 @@ def test_su2_simple_update_d24_matches_reference():
     for i, w in enumerate(su.get_weights()):
         np.testing.assert_allclose(w, d[f"w{i}"], rtol=1e-8, atol=1e-12)
     assert abs(su.logZ - float(d["logZ"])) < 1e-10
+
+
+@pytest.mark.parametrize("model", ["J1-J2", "checkerboard", "Shastry-Sutherland"])
+def test_second_neighbor_models_match_reference(model):
+    """square_lattice_second_neighbor (simple_update.py:366-407) with the U(1)
+    Heisenberg gates (J2 = 0.5, D = 4): beta, logZ, bond representations and
+    weights after each of two evolve steps equal the reference's run.  The
+    second-neighbour gates go through update_through_proxy
+    (simple_update.py:700-790)."""
+    from frostspin_b200 import U1SymmetricTensor
+    from frostspin_b200.simple_update import SimpleUpdate
+
+    d = load("simple_update_j1j2")
+    h1 = U1SymmetricTensor.load_from_dic(d, prefix="h1")
+    su = SimpleUpdate.square_lattice_second_neighbor(h1, 0.5 * h1, 4, 0.01, model=model,
+                                                     rcutoff=1e-10, degen_ratio=0.9999)
+    for k in range(2):
+        su.evolve(0.04)
+        assert abs(su.beta - float(d[f"{model}_b{k}_beta"])) < 1e-12
+        assert abs(su.logZ - float(d[f"{model}_b{k}_logZ"])) < 1e-10
+        for i, r in enumerate(su.get_bond_representations()):
+            assert np.array_equal(r, d[f"{model}_b{k}_rep{i}"]), (k, i)
+        for i, w in enumerate(su.get_weights()):
+            assert np.abs(w - d[f"{model}_b{k}_w{i}"]).max() < 1e-8, (k, i)
