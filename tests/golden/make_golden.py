@@ -518,6 +518,32 @@ def case_simple_update_j1j2():
     save("simple_update_j1j2", data)
 
 
+def case_symmetrized_simple_update():
+    """SymmetrizedSimpleUpdate (symmetrized_simple_update.py:10-271) of the
+    reference on the input of its tests/test_symmetrized_ctm.py (S.S in the
+    rotated basis, signature (0, 1, 1, 0), D = 7), tau = 0.01, two evolve
+    steps of 0.1: beta, logZ, bond representations and weights."""
+    from frostspin import SU2SymmetricTensor
+    from frostspin.simple_update import SymmetrizedSimpleUpdate
+
+    r2 = su2_rep([1], [2])
+    arrb = np.array([[-0.25, 0.0, 0.0, -0.5], [0.0, 0.25, 0.0, 0.0],
+                     [0.0, 0.0, 0.25, 0.0], [-0.5, 0.0, 0.0, -0.25]]).reshape(2, 2, 2, 2)
+    h = SU2SymmetricTensor.from_array(arrb, (r2, r2), (r2, r2), [0, 1, 1, 0])
+    data = {}
+    pack_tensor("h", h, data)
+    su = SymmetrizedSimpleUpdate.from_infinite_temperature(7, 0.01, [h])
+    for k in range(2):
+        su.evolve(0.1)
+        data[f"b{k}_beta"] = np.array(su.beta)
+        data[f"b{k}_logZ"] = np.array(su.logZ)
+        for i, w in enumerate(su.get_weights()):
+            data[f"b{k}_w{i}"] = w
+        for i, r in enumerate(su.get_bond_representations()):
+            data[f"b{k}_rep{i}"] = r
+    save("symmetrized_simple_update", data)
+
+
 def case_su2_d24_beta2():
     """Site tensors of the SU(2) CTMRG benchmark: the reference's SU(2) simple
     update of the Heisenberg model, D=24, tau=0.01, evolved to beta=2."""

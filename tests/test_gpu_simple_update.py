@@ -119,3 +119,27 @@ def test_second_neighbor_models_match_reference(model):
             assert np.array_equal(r, d[f"{model}_b{k}_rep{i}"]), (k, i)
         for i, w in enumerate(su.get_weights()):
             assert np.abs(w - d[f"{model}_b{k}_w{i}"]).max() < 1e-8, (k, i)
+
+
+def test_symmetrized_simple_update_matches_reference():
+    """SymmetrizedSimpleUpdate (symmetrized_simple_update.py:10-271) on the input
+    of the reference's tests/test_symmetrized_ctm.py (D = 7), tau = 0.01, two
+    evolve steps: beta, logZ, bond representations and weights equal the
+    reference's run; the tensors of the cell are A and its rotated dagger."""
+    from frostspin_b200 import SU2SymmetricTensor
+    from frostspin_b200.simple_update import SymmetrizedSimpleUpdate
+
+    d = load("symmetrized_simple_update")
+    h = SU2SymmetricTensor.load_from_dic(d, prefix="h")
+    su = SymmetrizedSimpleUpdate.from_infinite_temperature(7, 0.01, [h])
+    assert su.n_bonds == 4 and su.beta == 0.0
+    for k in range(2):
+        su.evolve(0.1)
+        assert abs(su.beta - float(d[f"b{k}_beta"])) < 1e-12
+        assert abs(su.logZ - float(d[f"b{k}_logZ"])) < 1e-10
+        for i, r in enumerate(su.get_bond_representations()):
+            assert np.array_equal(r, d[f"b{k}_rep{i}"]), (k, i)
+        for i, w in enumerate(su.get_weights()):
+            assert np.abs(w - d[f"b{k}_w{i}"]).max() < 1e-8, (k, i)
+    A, B = su.get_tensors()
+    assert (B - A.dagger().permute((4, 5), (2, 3, 0, 1))).norm() < 1e-14
