@@ -188,6 +188,8 @@ SIGNATURES = {
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "fs_ozaki_gemm_pair": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _I64, _P, _P]),
     "fs_ozaki_gemm_noalloc": (ctypes.c_int, [_P, _I64, _I32, _P]),
+    "fs_ozaki_noalloc_status": (ctypes.c_int, [_P, _P]),
+    "fs_set_spin_limit": (ctypes.c_int64, [_I64]),
     "fs_scale": (ctypes.c_int, [_P, _I64, _D, _P]),
     "fs_axpby": (ctypes.c_int, [_P, _P, _I64, _D, _D, _P]),
     "fs_scale_by": (ctypes.c_int, [_P, _I64, _P, _I32, _P]),

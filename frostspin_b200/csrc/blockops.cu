@@ -7,7 +7,9 @@
 namespace fsb {
 
 constexpr int kOpThreads = 256;
-constexpr int kReducePartials = 2 * kNumSM;
+// partial sums of the weighted reductions: a fixed count (two CTAs per SM of a
+// 148-SM B200) so that the caller-owned scratch size does not depend on the GPU
+constexpr int kReducePartials = 296;
 
 __global__ void k_scale(double* __restrict__ x, int64_t n, double alpha) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(kOpThreads)
 
 inline int elementwise_grid(int64_t n) {
     int64_t g = (n + kOpThreads - 1) / kOpThreads;
-    const int64_t cap = static_cast<int64_t>(kNumSM) * 16;
+    const int64_t cap = static_cast<int64_t>(num_sms()) * 16;
     if (g > cap) g = cap;
     if (g < 1) g = 1;
     return static_cast<int>(g);
@@ -252,7 +254,7 @@ extern "C" int fs_diag_mul(const double* d_x, const double* d_diag, double* d_ou
     if (n_blocks == 0) return FS_OK;
     if (d_x == nullptr || d_diag == nullptr || d_out == nullptr || d_blocks == nullptr)
         return FS_ERR_INVALID_ARG;
-    dim3 grid(fsb::kNumSM, static_cast<unsigned>(n_blocks < 65535 ? n_blocks : 65535));
+    dim3 grid(fsb::num_sms(), static_cast<unsigned>(n_blocks < 65535 ? n_blocks : 65535));
     fsb::k_diag_mul<<<grid, fsb::kOpThreads, 0, fsb::as_stream(stream)>>>(d_x, d_diag, d_out,
                                                                           d_blocks, n_blocks);
     return fsb::launch_status();

@@ -8,11 +8,21 @@
 
 namespace fsb {
 
-// Number of SMs on a B200; grids are sized as multiples of it.
-constexpr int kNumSM = 148;
-
 // Records the CUDA error string for fs_last_cuda_error (thread local).
 void set_last_cuda_error(cudaError_t err);
+
+// Number of SMs of the current device (queried once per device, cached);
+// grids are sized as multiples of it.  Falls back to 148 (B200) if the query
+// fails, so a grid is never empty.
+int num_sms();
+
+// Sets the dynamic shared memory limit of a kernel on the current device once
+// per device (the attribute is per device).  Returns FS_OK or FS_ERR_CUDA.
+int configure_smem(const void* func, int bytes);
+
+// Iteration bound of the abortable device waits of the tcgen05 kernels, in
+// clock64 cycles (fs_set_spin_limit).
+long long spin_limit();
 
 inline int launch_status() {
     cudaError_t err = cudaGetLastError();

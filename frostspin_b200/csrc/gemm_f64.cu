@@ -335,14 +335,10 @@ extern "C" int fs_grouped_dgemm(const FsGemmProblem* d_problems, int64_t n_probl
     if (n_tiles < 0 || n_problems < 0) return FS_ERR_INVALID_ARG;
     if (n_tiles == 0) return FS_OK;
     if (d_problems == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(fsb::k_grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(fsb::kGemmSmem)) != cudaSuccess)
-            return fsb::launch_status();
-        configured = true;
-    }
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 3;
+    const int cfg = fsb::configure_smem(reinterpret_cast<const void*>(fsb::k_grouped_dgemm),
+                                        static_cast<int>(fsb::kGemmSmem));
+    if (cfg != FS_OK) return cfg;
+    const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 3;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
     fsb::k_grouped_dgemm<<<grid, fsb::kGemmThreads, fsb::kGemmSmem, fsb::as_stream(stream)>>>(
         d_problems, n_problems, d_tiles, n_tiles);
@@ -354,15 +350,11 @@ namespace {
 template <bool TA, bool TB>
 int launch_stream(const FsGemmProblem* d_problems, int64_t n_problems, const FsGemmTile* d_tiles,
                   int64_t n_tiles, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(fsb::k_grouped_dgemm_stream<TA, TB>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(fsb::kGemmSmem)) != cudaSuccess)
-            return fsb::launch_status();
-        configured = true;
-    }
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 3;
+    const int cfg = fsb::configure_smem(
+        reinterpret_cast<const void*>(fsb::k_grouped_dgemm_stream<TA, TB>),
+        static_cast<int>(fsb::kGemmSmem));
+    if (cfg != FS_OK) return cfg;
+    const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 3;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
     fsb::k_grouped_dgemm_stream<TA, TB><<<grid, fsb::kGemmThreads, fsb::kGemmSmem, s>>>(
         d_problems, n_problems, d_tiles, n_tiles);
@@ -484,7 +476,7 @@ extern "C" int fs_grouped_dgemm_thin(const FsGemmProblem* d_problems, int64_t n_
     if (n_tiles < 0 || n_problems < 0) return FS_ERR_INVALID_ARG;
     if (n_tiles == 0) return FS_OK;
     if (d_problems == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 8;
+    const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 8;
     const int grid = static_cast<int>(n_tiles < max_grid ? n_tiles : max_grid);
     fsb::k_grouped_dgemm_thin<<<grid, fsb::kThinThreads, 0, fsb::as_stream(stream)>>>(
         d_problems, n_problems, d_tiles, n_tiles);
@@ -523,7 +515,7 @@ extern "C" int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items,
     if (d_items == nullptr) return FS_ERR_INVALID_ARG;
     if (n_items > 65535) return FS_ERR_TOO_LARGE;
     const int64_t blocks = (max_elems + 255) / 256;
-    const int gx = static_cast<int>(blocks < 4 * fsb::kNumSM ? blocks : 4 * fsb::kNumSM);
+    const int gx = static_cast<int>(blocks < 4 * fsb::num_sms() ? blocks : 4 * fsb::num_sms());
     fsb::k_splitk_reduce<<<dim3(gx, static_cast<unsigned>(n_items)), 256, 0,
                            fsb::as_stream(stream)>>>(d_items, n_items);
     return fsb::launch_status();

@@ -44,7 +44,10 @@ constexpr int kStageBytes = kABytes + kBBytes;      // 48 KB
 constexpr int kThreads = 192;                       // 6 warps
 constexpr int kTmemCols = 512;                      // two 256-column accumulators
 constexpr int kSplitRows = 128;                     // rows per slice tile
-constexpr long long kSpinLimit = 2000000000LL;      // ~1 s of clock64 at 1.9 GHz
+// bound of the waits that drain in-flight copies and MMAs on the way out
+// (~1 s of clock64 at 1.9 GHz); the abortable waits use the runtime bound
+// passed to each kernel (fs_set_spin_limit)
+constexpr long long kDrainLimit = 2000000000LL;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -78,11 +81,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 
 // Bounded wait: false on timeout or when another role already aborted.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
-                                          volatile int* abort_flag) {
+                                          volatile int* abort_flag, long long limit) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort_flag) return false;
-        if (clock64() - t0 > kSpinLimit) {
+        if (clock64() - t0 > limit) {
             *abort_flag = 1;
             return false;
         }
@@ -94,7 +97,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
 __device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kSpinLimit) return false;
+        if (clock64() - t0 > kDrainLimit) return false;
     }
     return true;
 }
@@ -249,7 +252,7 @@ struct PassIter {
 __global__ void __launch_bounds__(kThreads, 1)
     k_oz_gemm(const FsOzProblem* __restrict__ probs, int64_t n_probs,
               const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
-              int chunk_ktiles, int32_t* flag) {
+              int chunk_ktiles, int32_t* flag, long long spin) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             const int tt = d - s;
                             for (int kt = k0; kt < k1; ++kt) {
                                 if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1,
-                                               abort_flag)) {
+                                               abort_flag, spin)) {
                                     ok = false;
                                     break;
                                 }
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
                         const int k1 = min(p.ktiles, k0 + chunk_ktiles);
                         if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1,
-                                       abort_flag)) {
+                                       abort_flag, spin)) {
                             ok = false;
                             break;
                         }
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         uint32_t accumulate = 0;
                         for (int s = 0; ok && s <= d; ++s) {
                             for (int kt = k0; kt < k1; ++kt) {
-                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
+                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag, spin)) {
                                     ok = false;
                                     break;
                                 }
@@ -413,7 +416,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     // warp-wide tcgen05.ld below is never reached by a subset
                     int got = 0;
                     if (lane == 0)
-                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag)
+                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag, spin)
                                   ? 1
                                   : 0;
                     got = __shfl_sync(0xffffffffu, got, 0);
@@ -589,7 +592,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     k_oz_gemm_pair(const FsOzProblem* __restrict__ probs, int64_t n_probs,
                    const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
                    int chunk_ktiles, int32_t* flag, const __grid_constant__ CUtensorMap ws_map,
-                   const int8_t* ws_base) {
+                   const int8_t* ws_base, long long spin) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -647,7 +650,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         for (int s = 0; ok && s <= d; ++s) {
                             for (int kt = k0; kt < k1; ++kt) {
                                 if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1,
-                                               abort_flag)) {
+                                               abort_flag, spin)) {
                                     ok = false;
                                     break;
                                 }
@@ -699,7 +702,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
                         const int k1 = min(p.ktiles, k0 + chunk_ktiles);
                         if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1,
-                                       abort_flag)) {
+                                       abort_flag, spin)) {
                             ok = false;
                             break;
                         }
@@ -708,7 +711,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         uint32_t accumulate = 0;
                         for (int s = 0; ok && s <= d; ++s) {
                             for (int kt = k0; kt < k1; ++kt) {
-                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag)) {
+                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag, spin)) {
                                     ok = false;
                                     break;
                                 }
@@ -762,7 +765,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
                     int got = 0;
                     if (lane == 0)
-                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag)
+                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag, spin)
                                   ? 1
                                   : 0;
                     got = __shfl_sync(0xffffffffu, got, 0);
@@ -852,12 +855,12 @@ extern "C" int fs_ozaki_split(const FsOzOperand* d_ops, int64_t n_ops, int32_t m
     if (n_ops > 65535) return FS_ERR_TOO_LARGE;
     cudaStream_t s = fsb::as_stream(stream);
     const int gx = static_cast<int>(
-        ((max_rows + 7) / 8) < 4 * fsb::kNumSM ? ((max_rows + 7) / 8) : 4 * fsb::kNumSM);
+        ((max_rows + 7) / 8) < 4 * fsb::num_sms() ? ((max_rows + 7) / 8) : 4 * fsb::num_sms());
     fsb::oz::k_oz_exponents<<<dim3(gx > 0 ? gx : 1, static_cast<unsigned>(n_ops)), 256, 0, s>>>(
         d_ops, n_ops);
     int st = fsb::launch_status();
     if (st != FS_OK) return st;
-    const int tx = max_tiles < 4 * fsb::kNumSM ? max_tiles : 4 * fsb::kNumSM;
+    const int tx = max_tiles < 4 * fsb::num_sms() ? max_tiles : 4 * fsb::num_sms();
     fsb::oz::k_oz_split<<<dim3(tx, static_cast<unsigned>(n_ops)), 1024, 0, s>>>(d_ops, n_ops,
                                                                                 nslices);
     return fsb::launch_status();
@@ -876,19 +879,11 @@ extern "C" int fs_ozaki_gemm(const FsOzProblem* d_probs, int64_t n_probs,
     if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
     const int smem = fsb::oz::kStages * fsb::oz::kStageBytes +
                      static_cast<int>(sizeof(fsb::oz::Barriers)) + 1024;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fsb::oz::k_oz_gemm,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) {
-            fsb::set_last_cuda_error(e);
-            return FS_ERR_CUDA;
-        }
-        configured = true;
-    }
-    const int grid = static_cast<int>(n_tiles < fsb::kNumSM ? n_tiles : fsb::kNumSM);
+    const int cfg = fsb::configure_smem(reinterpret_cast<const void*>(fsb::oz::k_oz_gemm), smem);
+    if (cfg != FS_OK) return cfg;
+    const int grid = static_cast<int>(n_tiles < fsb::num_sms() ? n_tiles : fsb::num_sms());
     fsb::oz::k_oz_gemm<<<grid, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
-        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag);
+        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag, fsb::spin_limit());
     return fsb::launch_status();
 }
 
@@ -945,21 +940,14 @@ extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
     if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
     const int smem = fsb::oz::kPairStages * fsb::oz::kPairStageBytes +
                      static_cast<int>(sizeof(fsb::oz::PairBarriers)) + 1024;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fsb::oz::k_oz_gemm_pair,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) {
-            fsb::set_last_cuda_error(e);
-            return FS_ERR_CUDA;
-        }
-        configured = true;
-    }
-    const int64_t max_clusters = fsb::kNumSM / 2;
+    const int cfg =
+        fsb::configure_smem(reinterpret_cast<const void*>(fsb::oz::k_oz_gemm_pair), smem);
+    if (cfg != FS_OK) return cfg;
+    const int64_t max_clusters = fsb::num_sms() / 2;
     const int clusters = static_cast<int>(n_tiles < max_clusters ? n_tiles : max_clusters);
     fsb::oz::k_oz_gemm_pair<<<2 * clusters, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
         d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag, map,
-        static_cast<const int8_t*>(d_workspace));
+        static_cast<const int8_t*>(d_workspace), fsb::spin_limit());
     return fsb::launch_status();
 }
 
@@ -977,6 +965,7 @@ extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(48) << 20;   // 48 MiB
+constexpr int64_t kNoAllocStatusBytes = 256;   // status word, padded to keep slices aligned
 constexpr int kNoAllocMaxDevices = 64;
 
 std::mutex g_noalloc_mutex;
@@ -1024,12 +1013,23 @@ extern "C" int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_
         return FS_ERR_INVALID_ARG;
     if (n_problems == 0) return FS_OK;
     if (h_problems == nullptr) return FS_ERR_INVALID_ARG;
+    cudaStream_t s = fsb::as_stream(stream);
+    // the launch tables are staged from host memory that is gone when this
+    // call returns: a captured copy would replay from freed memory
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(s, &capturing);
+    if (ce != cudaSuccess) {
+        fsb::set_last_cuda_error(ce);
+        return FS_ERR_CUDA;
+    }
+    if (capturing != cudaStreamCaptureStatusNone) return FS_ERR_UNSUPPORTED;
 
-    // layout of the scratch: per problem slices and exponents, then the tables
+    // layout of the scratch: the status word, per problem slices and
+    // exponents, then the tables
     std::vector<FsOzOperand> ops;
     std::vector<FsOzProblem> probs;
     std::vector<std::pair<int32_t, FsOzTile>> tiles;  // (K, tile) for ordering
-    int64_t off = 0;
+    int64_t off = kNoAllocStatusBytes;
     int32_t max_rows = 0, max_tiles = 0;
     for (int64_t i = 0; i < n_problems; ++i) {
         const FsGemmProblem& g = h_problems[i];
@@ -1101,11 +1101,17 @@ extern "C" int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_
     FsOzTile* tdst = reinterpret_cast<FsOzTile*>(staging.data() + (tiles_off - ops_off));
     for (size_t i = 0; i < tiles.size(); ++i) tdst[i] = tiles[i].second;
 
-    cudaStream_t s = fsb::as_stream(stream);
+    // the status word starts every call at zero; a bounded device wait that
+    // runs out writes FS_ERR_TIMEOUT into it (fs_ozaki_noalloc_status)
+    int32_t* d_status = reinterpret_cast<int32_t*>(base);
+    cudaError_t e = cudaMemsetAsync(d_status, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) {
+        fsb::set_last_cuda_error(e);
+        return FS_ERR_CUDA;
+    }
     // pageable source: the call returns once the bytes are staged, so the
     // host vectors may go out of scope afterwards
-    cudaError_t e = cudaMemcpyAsync(base + ops_off, staging.data(), staging.size(),
-                                    cudaMemcpyHostToDevice, s);
+    e = cudaMemcpyAsync(base + ops_off, staging.data(), staging.size(), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
         fsb::set_last_cuda_error(e);
         return FS_ERR_CUDA;
@@ -1122,5 +1128,19 @@ extern "C" int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_
     return fs_ozaki_gemm(reinterpret_cast<const FsOzProblem*>(base + probs_off),
                          static_cast<int64_t>(probs.size()),
                          reinterpret_cast<const FsOzTile*>(base + tiles_off),
-                         static_cast<int64_t>(tiles.size()), nslices, chunk, nullptr, stream);
+                         static_cast<int64_t>(tiles.size()), nslices, chunk, d_status, stream);
+}
+
+extern "C" int fs_ozaki_noalloc_status(void* stream, int32_t* status) {
+    if (status == nullptr) return FS_ERR_INVALID_ARG;
+    uint8_t* base = nullptr;
+    int st = noalloc_scratch(&base);
+    if (st != FS_OK) return st;
+    cudaError_t e = cudaStreamSynchronize(fsb::as_stream(stream));
+    if (e == cudaSuccess) e = cudaMemcpy(status, base, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        fsb::set_last_cuda_error(e);
+        return FS_ERR_CUDA;
+    }
+    return FS_OK;
 }

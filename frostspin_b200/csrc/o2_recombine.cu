@@ -79,7 +79,7 @@ extern "C" int fs_o2_recombine(const double* d_src, int64_t src_len, double* d_o
         return FS_ERR_INVALID_ARG;
     if (d_src == nullptr && src_len > 0) return FS_ERR_INVALID_ARG;
     if (n_blocks > 65535) return FS_ERR_TOO_LARGE;
-    const int64_t cap = static_cast<int64_t>(fsb::kNumSM) * 8;
+    const int64_t cap = static_cast<int64_t>(fsb::num_sms()) * 8;
     const int gx = static_cast<int>(max_rows < cap ? max_rows : cap);
     fsb::k_o2_recombine<<<dim3(gx, static_cast<unsigned>(n_blocks)), fsb::kO2Threads, 0,
                           fsb::as_stream(stream)>>>(d_src, src_len, d_out, out_len, d_blocks,

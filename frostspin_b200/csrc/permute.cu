@@ -118,7 +118,7 @@ extern "C" int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_
     if (d_out == nullptr || d_ebs == nullptr || d_tasks == nullptr) return FS_ERR_INVALID_ARG;
     if (d_in == nullptr && in_len > 0) return FS_ERR_INVALID_ARG;
     // one wave of resident CTAs (4 per SM at the kernel's register budget)
-    const int64_t max_grid = static_cast<int64_t>(fsb::kNumSM) * 4;
+    const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 4;
     const int grid = static_cast<int>(n_tasks < max_grid ? n_tasks : max_grid);
     fsb::k_perm_gather<<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
         d_in, in_len, d_out, out_len, d_ebs, n_ebs, d_tasks, n_tasks, d_flag);

@@ -44,6 +44,16 @@ const char* fs_status_string(int status);
 /* Name of the last CUDA error seen by this library on the calling thread. */
 const char* fs_last_cuda_error(void);
 
+/*
+ * Bound, in clock64 cycles, of every device wait of the tcgen05 kernels that
+ * ends in FS_ERR_TIMEOUT (default 2e9, about one second); cycles <= 0 restores
+ * the default.  Returns the previous bound.  Kernels launched afterwards use
+ * the new bound; the waits that drain in-flight copies and MMAs before a
+ * kernel returns keep the default.  No counterpart in the reference (which has
+ * no device code); it exists so that the timeout path can be exercised.
+ */
+int64_t fs_set_spin_limit(int64_t cycles);
+
 /* --------------------------------------------------------- abelian permute */
 /*
  * An elementary block (EB) is the set of tensor entries whose legs each lie in
@@ -262,23 +272,34 @@ int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
  * would fail or fragment that pool), or a C / Fortran driver without a device
  * allocator that only holds its input and output buffers.  The caller passes
  * the problems as a HOST array of FsGemmProblem (same meaning as for
- * fs_grouped_dgemm; A, B and C are device pointers).  Digit slices, exponents
- * and launch tables go to a fixed 48 MiB file-scope device array inside this
- * library, which every GPU that loads the library holds until the process
- * exits; requests that do not fit return FS_ERR_TOO_LARGE before any GPU work
- * (one 1024^3 product with 7 slices needs about 15 MiB).
+ * fs_grouped_dgemm; A, B and C are device pointers).  Digit slices, exponents,
+ * launch tables and a status word go to a fixed 48 MiB file-scope device array
+ * inside this library, which every GPU that loads the library holds until the
+ * process exits; requests that do not fit return FS_ERR_TOO_LARGE before any
+ * GPU work (one 1024^3 product with 7 slices needs about 15 MiB).
  *
  * The first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture.  The call
- * copies its launch tables from host memory with cudaMemcpyAsync and calls no
- * cudaMalloc, cudaFree or allocating library routine.  All calls on a device
- * share that device's array and every call rewrites what it reads, so calls
- * that overlap on the GPU (for example on two streams of the same device) race;
- * serialise them.  A bounded device wait that runs out ends the kernel early but
- * is not reported through this entry point.
+ * device current).  The call copies its launch tables from host memory with
+ * cudaMemcpyAsync and calls no cudaMalloc, cudaFree or allocating library
+ * routine.  It must not be called while `stream` is being captured into a CUDA
+ * graph (the staged host tables do not outlive the call): it returns
+ * FS_ERR_UNSUPPORTED then.  All calls on a device share that device's array and
+ * every call rewrites what it reads, so calls that overlap on the GPU (for
+ * example on two streams of the same device) race; serialise them.
+ *
+ * A bounded device wait that runs out ends the kernel early and leaves C
+ * partly written; it is reported through fs_ozaki_noalloc_status.
  */
 int fs_ozaki_gemm_noalloc(const FsGemmProblem* h_problems, int64_t n_problems,
                           int32_t nslices, void* stream);
+
+/*
+ * Status of the last fs_ozaki_gemm_noalloc call on the current device: waits
+ * for `stream` to finish, then copies the status word of the fixed array to
+ * *status (FS_OK, or FS_ERR_TIMEOUT when a bounded device wait ran out).
+ * Allocates nothing.  No counterpart in the reference.
+ */
+int fs_ozaki_noalloc_status(void* stream, int32_t* status);
 
 /* -------------------------------------------------------------- block ops */
 /* x[0:n] *= alpha.  Replaces SymmetricTensor.__imul__/__itruediv__

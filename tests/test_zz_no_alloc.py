@@ -58,12 +58,22 @@ def run_noalloc(problems, dev):
     outs = [torch.full((A.shape[0], B.shape[1]), np.nan, dtype=torch.float64, device="cuda")
             for A, B, _, _ in problems]
     arr = problem_table(problems, dev, outs)
-    st = _native.lib().fs_ozaki_gemm_noalloc(
-        arr.ctypes.data, arr.size, SLICES, torch.cuda.current_stream().cuda_stream
-    )
+    stream = torch.cuda.current_stream().cuda_stream
+    st = _native.lib().fs_ozaki_gemm_noalloc(arr.ctypes.data, arr.size, SLICES, stream)
     assert st == 0, _native.lib().fs_status_string(st)
+    assert noalloc_status(stream) == 0
     torch.cuda.synchronize()
     return [c.cpu().numpy() for c in outs]
+
+
+def noalloc_status(stream):
+    import ctypes
+
+    from frostspin_b200 import _native
+
+    status = ctypes.c_int32(99)
+    assert _native.lib().fs_ozaki_noalloc_status(stream, ctypes.byref(status)) == 0
+    return status.value
 
 
 def run_workspace(problems, dev):
@@ -109,3 +119,59 @@ def test_noalloc_rejects_requests_beyond_its_scratch():
     st = _native.lib().fs_ozaki_gemm_noalloc(arr.ctypes.data, 1, 8, None)
     assert st == -7  # FS_ERR_TOO_LARGE
     assert _native.lib().fs_ozaki_gemm_noalloc(arr.ctypes.data, 1, 0, None) == -1
+
+
+def test_noalloc_reports_a_wait_that_ran_out():
+    """With the wait bound cut to one cycle the kernel's first wait runs out:
+    the kernel drains its copies and returns early, and the status query (not
+    the call's return value, which only covers the launch) reports
+    FS_ERR_TIMEOUT.  With the default bound restored the next call is exact."""
+    import torch
+
+    from frostspin_b200 import _native
+
+    rng = np.random.default_rng(7)
+    problems = make_problems(rng)[:3]
+    dev = device_operands(problems)
+    outs = [torch.zeros((A.shape[0], B.shape[1]), dtype=torch.float64, device="cuda")
+            for A, B, _, _ in problems]
+    arr = problem_table(problems, dev, outs)
+    stream = torch.cuda.current_stream().cuda_stream
+    lib = _native.lib()
+    old = lib.fs_set_spin_limit(1)
+    try:
+        assert lib.fs_ozaki_gemm_noalloc(arr.ctypes.data, arr.size, SLICES, stream) == 0
+        assert noalloc_status(stream) == -4  # FS_ERR_TIMEOUT
+    finally:
+        lib.fs_set_spin_limit(old)
+    got = run_noalloc(problems, dev)
+    ref = run_workspace(problems, dev)
+    for g, r in zip(got, ref, strict=True):
+        assert np.array_equal(g, r)
+
+
+def test_noalloc_refuses_stream_capture():
+    """The staged host tables do not outlive a call, so a call on a stream that
+    is being captured is refused before anything is enqueued."""
+    import torch
+
+    from frostspin_b200 import _native
+
+    rng = np.random.default_rng(8)
+    problems = make_problems(rng)[:1]
+    dev = device_operands(problems)
+    outs = [torch.zeros((A.shape[0], B.shape[1]), dtype=torch.float64, device="cuda")
+            for A, B, _, _ in problems]
+    arr = problem_table(problems, dev, outs)
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        try:
+            st = _native.lib().fs_ozaki_gemm_noalloc(arr.ctypes.data, arr.size, SLICES,
+                                                     s.cuda_stream)
+            outs[0].add_(0.0)  # keep the captured graph non-empty
+        finally:
+            g.capture_end()
+    assert st == -5  # FS_ERR_UNSUPPORTED
