@@ -2,7 +2,7 @@
 """Benchmark driver: prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ctmrg|u1_microbench|gemm] [--precision fp64|ozakiS]
+                    [--workload ctmrg|u1_microbench|gemm|ising] [--precision fp64|ozakiS|ozaki2_N]
 
 Workload "ctmrg" (default): double-layer CTMRG of the spin-1/2 Heisenberg
 model on the square lattice.  The site tensors come from the finite-temperature
@@ -214,15 +214,26 @@ def measure_dgemm_peak():
     return best
 
 
-def tensor_ops_ozaki(p, t2, S):
-    """int8 tensor-core operations the Ozaki path issues: S(S+1)/2 slice products
-    of 2 M N K each on the padded tile grid (128 x 256 x 128)."""
+def tensor_ops_ozaki(p, t2, precision):
+    """int8 tensor-core operations the mixed path issues on the padded tile
+    grid: S(S+1)/2 digit-slice products of 2 M N K (ozakiS, 128 x 256 x 128
+    tiles) or one product per modulus (ozaki2_N, 256 x 256 x 128 tiles)."""
     common, i1, i2 = np.intersect1d(p.block_irreps, t2.block_irreps, return_indices=True)
     m = p.block_shapes[i1, 0]
     k = p.block_shapes[i1, 1]
     n = t2.block_shapes[i2, 1]
     pad = lambda x, a: (x + a - 1) // a * a  # noqa: E731
+    if precision.startswith("ozaki2_"):
+        nmod = int(precision[7:])
+        return float((2 * pad(m, 256) * pad(n, 256) * pad(k, 128)).sum() * nmod)
+    S = int(precision[5:])
     return float((2 * pad(m, 128) * pad(n, 256) * pad(k, 128)).sum() * S * (S + 1) // 2)
+
+
+def mixed_kernel_names(precision):
+    if precision.startswith("ozaki2_"):
+        return "k_oz_pair<CRT> (+ k_oz2_split, k_oz2_exponents)"
+    return "k_oz_pair / k_oz_gemm (+ k_oz_split, k_oz_exponents)"
 
 
 # --------------------------------------------------------------- CPU baseline
@@ -427,7 +438,7 @@ def run_ctmrg(args, world, rank, local):
     perm = kern.get("permute", {"ms": 1.0, "bytes": 0.0, "launches": 0})
     if headline_mixed and "gemm_ozaki" in kern:
         ach = gem["int8_ops"] / (gem["ms"] * 1e-3) / 1e12
-        roof = {"bound": "tensor", "kernel": "k_oz_gemm (+ k_oz_split, k_oz_exponents)",
+        roof = {"bound": "tensor", "kernel": mixed_kernel_names(mixed),
                 "achieved": ach, "peak": 2.0 * bf16, "unit": "TOP/s (int8)",
                 "frac": ach / (2.0 * bf16),
                 "peak_kind": f"2 x {peak_kind} bf16 dense (int8 dense rate is twice bf16)",
@@ -704,12 +715,11 @@ def run_ours(args, world, rank, local):
     gemm_tf = flops / (gemm_ms * 1e-3) / 1e12
     value = world * args.steps / elapsed
     if args.precision.startswith("ozaki"):
-        S = int(args.precision[5:])
-        int8_ops = tensor_ops_ozaki(t1.permute((0, 2), (1, 3)), t2, S)
+        int8_ops = tensor_ops_ozaki(t1.permute((0, 2), (1, 3)), t2, args.precision)
         int8_peak = 2.0 * bf16
         gemm_roofline = {
             "bound": "tensor",
-            "kernel": "k_oz_gemm",
+            "kernel": mixed_kernel_names(args.precision),
             "achieved": int8_ops / (gemm_ms * 1e-3) / 1e12,
             "peak": int8_peak,
             "unit": "TOP/s (int8)",
@@ -858,11 +868,105 @@ def run_reference_ctmrg(args, world):
     }
 
 
+ISING_BETA = 0.44
+ISING_CHI = 32
+ISING_ITERS = 100
+
+
+def run_ising(args, world, rank, local):
+    """Config 1: C4v classical Ising CTMRG (Z2 sectors), beta = 0.44, chi = 32,
+    the reference example's seeded start; one step = one iteration
+    (examples/ising_classical_ctmrg.py:115-204).  W untimed then K timed
+    iterations, then untimed iterations up to 100 in total, after which the
+    energy per bond and the correlation length are reported."""
+    import torch
+
+    from frostspin_b200 import _native
+    from frostspin_b200.ctmrg import (correlation_length, energy_per_bond,
+                                      ising_initial_environment, ising_site_tensors,
+                                      iterate_c4v)
+
+    a, a2, a0d, mopd = ising_site_tensors(ISING_BETA)
+    s, T = ising_initial_environment(ISING_CHI, np.random.default_rng(42))
+    for _ in range(args.warmup):
+        s, T = iterate_c4v(s, T, a, a2, ISING_CHI)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = _native.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        s, T = iterate_c4v(s, T, a, a2, ISING_CHI)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = _native.kernel_launches() - n0
+    clk = clocks.stop()
+    t = max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, world)
+    done = args.warmup + args.steps
+    for _ in range(max(0, ISING_ITERS - done)):
+        s, T = iterate_c4v(s, T, a, a2, ISING_CHI)
+    e = energy_per_bond(s, T, a0d, mopd)
+    xi = correlation_length(T)
+    line = {
+        "metric": "C4v Ising CTMRG iter/s (chi=32)", "value": world * args.steps / t,
+        "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference example's seeded start)", "impl": "ours",
+        "config": {"workload": "ising_c4v", "beta": ISING_BETA, "chi": ISING_CHI,
+                   "iterations_total": max(done, ISING_ITERS),
+                   "energy_per_bond": e, "correlation_length": xi,
+                   "l2": "blocks of at most 16 x 32: launch-bound, L2-resident",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_ising_sample(max(args.steps, 20))
+    return line
+
+
+def cpu_ising_sample(n):
+    """The oracle's C4v iteration (numpy restatement of the reference example)
+    from the same seeded start, one BLAS thread: mean time of n iterations
+    after 3."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import frostspin_oracle as fo
+
+    a, a2, _, _ = fo.ising_tensors(ISING_BETA)
+    sb, si, T = fo.ising_initial_env(ISING_CHI, np.random.default_rng(42))
+    with threadpool_limits(limits=1):
+        for _ in range(3):
+            sb, si, T = fo.ising_c4v_iteration(sb, si, T, a, a2, ISING_CHI)
+        t0 = time.perf_counter()
+        for _ in range(n):
+            sb, si, T = fo.ising_c4v_iteration(sb, si, T, a, a2, ISING_CHI)
+        t = (time.perf_counter() - t0) / n
+    return {"value": 1.0 / t, "unit": "iter/s", "cores": 1, "kind": "port",
+            "sample": f"numpy oracle C4v iteration, chi={ISING_CHI}, mean of {n} after 3: "
+                      f"{t * 1e3:.2f} ms/iteration"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
     if args.workload == "ctmrg":
         return run_reference_ctmrg(args, world)
+    if args.workload == "ising":
+        info = cpu_ising_sample(max(args.steps, 20))
+        v = info["value"]
+        return {"metric": "C4v Ising CTMRG iter/s (chi=32)", "value": v, "unit": "iter/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference", "config": {"workload": "ising_c4v", "beta": ISING_BETA,
+                                                "chi": ISING_CHI},
+                "cpu_baseline": info,
+                "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     if args.workload == "gemm":
         rng = np.random.default_rng(SEED)
         n = args.gemm_n
@@ -935,7 +1039,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ctmrg", "u1_microbench", "gemm"], default="ctmrg")
+    ap.add_argument("--workload", choices=["ctmrg", "u1_microbench", "gemm", "ising"],
+                    default="ctmrg")
     ap.add_argument("--gemm-n", type=int, default=4096, help="matrix size of the gemm workload")
     ap.add_argument("--symmetry", choices=["u1", "su2"], default="su2")
     ap.add_argument("--D", type=int, default=None,
@@ -947,7 +1052,8 @@ def main():
     ap.add_argument("--ozaki-pair", choices=["on", "off"], default="on",
                     help="large int8 sector GEMMs on CTA pairs (tcgen05 cta_group::2)")
     ap.add_argument("--precision", default="ozaki7",
-                    help="sector GEMM arithmetic: fp64 or ozakiS (S = 3..8 int8 slices)")
+                    help="sector GEMM arithmetic: fp64, ozakiS (S = 3..8 int8 digit slices) "
+                         "or ozaki2_N (N = 8..14 int8 moduli, CRT)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
                     help="states per leg (256 = the benchmark; smaller for profiling)")
     args = ap.parse_args()
@@ -972,6 +1078,8 @@ def main():
         line = run_ctmrg(args, world, rank, local)
     elif args.workload == "gemm":
         line = run_gemm(args, world, rank, local)
+    elif args.workload == "ising":
+        line = run_ising(args, world, rank, local)
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0:

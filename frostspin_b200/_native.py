@@ -113,6 +113,47 @@ OZ_TILE_DTYPE = np.dtype([("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pa
 
 FS_OZAKI_MAX_SLICES = 8
 
+OZ2_OPERAND_DTYPE = np.dtype(
+    [
+        ("src", "<u8"),
+        ("s_row", "<i8"),
+        ("s_k", "<i8"),
+        ("slices", "<u8"),
+        ("exps", "<u8"),
+        ("rows", "<i4"),
+        ("K", "<i4"),
+        ("rowtiles", "<i4"),
+        ("ktiles", "<i4"),
+        ("bits", "<i4"),
+        ("pad", "<i4"),
+    ]
+)
+
+OZ2_PROBLEM_DTYPE = np.dtype(
+    [
+        ("a_slices", "<u8"),
+        ("b_slices", "<u8"),
+        ("a_exps", "<u8"),
+        ("b_exps", "<u8"),
+        ("C", "<u8"),
+        ("ldc", "<i8"),
+        ("M", "<i4"),
+        ("N", "<i4"),
+        ("K", "<i4"),
+        ("a_rowtiles", "<i4"),
+        ("b_rowtiles", "<i4"),
+        ("ktiles", "<i4"),
+        ("alpha", "<f8"),
+        ("beta", "<f8"),
+        ("a_bits", "<i4"),
+        ("b_bits", "<i4"),
+    ]
+)
+
+FS_OZAKI2_MIN_MODULI = 8
+FS_OZAKI2_MAX_MODULI = 14
+FS_OZAKI2_MAX_K = 131071
+
 SEGMENT_DTYPE = np.dtype([("offset", "<i8"), ("length", "<i8"), ("weight", "<f8")])
 
 PAIR_BLOCK_DTYPE = np.dtype(
@@ -187,6 +228,11 @@ SIGNATURES = {
     "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
     "fs_ozaki_gemm_pair": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _I64, _P, _P]),
+    "fs_ozaki2_bits": (ctypes.c_int, [_I32, _I64, _P, _P]),
+    "fs_ozaki2_constants": (ctypes.c_int, [_I32, _P, _P, _P, _P, _P, _P]),
+    "fs_ozaki2_scratch_bytes": (ctypes.c_int, [_I32, _P]),
+    "fs_ozaki2_split": (ctypes.c_int, [_P, _I64, _I32, _I64, _I32, _P]),
+    "fs_ozaki2_gemm_pair": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _P, _I64, _P, _I64, _P, _P]),
     "fs_ozaki_gemm_noalloc": (ctypes.c_int, [_P, _I64, _I32, _P]),
     "fs_ozaki_noalloc_status": (ctypes.c_int, [_P, _P]),
     "fs_set_spin_limit": (ctypes.c_int64, [_I64]),
@@ -244,7 +290,7 @@ CALL_COUNTS = {}
 LAUNCHES_PER_CALL = {
     "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
     "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2,
-    "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1,
+    "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1, "fs_ozaki2_split": 2, "fs_ozaki2_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
     "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1, "fs_o2_recombine": 1,
 }
@@ -279,3 +325,30 @@ def thin_dgemm_shape():
     tn = ctypes.c_int32()
     call("fs_thin_dgemm_shape", ctypes.byref(mm), ctypes.byref(mk), ctypes.byref(tn))
     return mm.value, mk.value, tn.value
+
+
+def ozaki2_bits(nmod, K):
+    """(a, b): operand bits the library uses for nmod moduli and inner size K."""
+    a = ctypes.c_int32()
+    b = ctypes.c_int32()
+    call("fs_ozaki2_bits", nmod, int(K), ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+def ozaki2_constants(nmod):
+    """The library's CRT constants (for checking against an exact computation)."""
+    moduli = np.zeros(nmod, dtype=np.int32)
+    w1 = np.zeros(nmod)
+    w2 = np.zeros(nmod)
+    pp = np.zeros(2)
+    frac = np.zeros(nmod, dtype=np.float32)
+    grids = np.zeros(2, dtype=np.int32)
+    call("fs_ozaki2_constants", nmod, moduli.ctypes.data, w1.ctypes.data, w2.ctypes.data,
+         pp.ctypes.data, frac.ctypes.data, grids.ctypes.data)
+    return {"moduli": moduli, "w1": w1, "w2": w2, "P": pp, "frac": frac, "grids": grids}
+
+
+def ozaki2_scratch_bytes(nmod):
+    n = ctypes.c_int64()
+    call("fs_ozaki2_scratch_bytes", nmod, ctypes.byref(n))
+    return n.value

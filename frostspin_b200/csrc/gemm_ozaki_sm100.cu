@@ -24,6 +24,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <utility>
@@ -484,13 +485,23 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ------------------------------------------------------- CTA-pair GEMM kernel
 //
-// The same arithmetic on 256 x 256 output tiles, computed by a cluster of two
-// CTAs with tcgen05.mma.cta_group::2 (M = 256, N = 256).  CTA r of the pair
-// loads its own 128 rows of the A slice tile (row tile 2 tm + r) and its own
-// 128 rows of the B^T slice tile (row tile 2 tn + r) into its own shared
-// memory: half the bytes per SM of the single-CTA kernel for the same MMA work.
-// The even CTA issues the MMAs, which read A from each CTA and B from both, and
-// accumulate rows [128 r, 128 r + 128) of the tile in CTA r's TMEM.
+// 256 x 256 output tiles computed by a cluster of two CTAs with
+// tcgen05.mma.cta_group::2 (M = 256, N = 256).  CTA r of the pair loads its
+// own 128 rows of the A slice tile (row tile 2 tm + r) and its own 128 rows of
+// the B^T slice tile (row tile 2 tn + r) into its own shared memory: half the
+// bytes per SM of the single-CTA kernel for the same MMA work.  The even CTA
+// issues the MMAs, which read A from each CTA and B from both, and accumulate
+// rows [128 r, 128 r + 128) of the tile in CTA r's TMEM.
+//
+// One kernel body serves both arithmetics (template kCRT):
+//   digits (Ozaki I): accumulator groups are (diagonal d, K chunk), each the
+//     sum over the slice pairs (s, d - s); the epilogue adds
+//     2^(ea + eb - 7(d+2)) * acc into C in FP64;
+//   moduli (Ozaki II): one accumulator group per modulus p_m, the product of
+//     the residue slices m of A and B over all of K; the epilogue reduces it
+//     to the symmetric residue mod p_m and parks it (one byte per entry) in a
+//     per-CTA scratch; after the last modulus the CRT reconstruction turns the
+//     residues into FP64 and writes C.
 //
 // Operand tiles are fetched by TMA through a 2-D tensor map that views the
 // slice workspace as rows of 128 bytes (box 128 x 128, no swizzle: the split
@@ -501,18 +512,26 @@ __global__ void __launch_bounds__(kThreads, 1)
 //                CTA arrives once with the expected byte count);
 //   empty[s]     both CTAs: the MMAs reading stage s finished (the even CTA's
 //                commit arrives on both CTAs' barriers);
-//   acc_full[b]  both CTAs: accumulator b holds a finished diagonal chunk;
+//   acc_full[b]  both CTAs: accumulator b holds a finished group;
 //   acc_empty[b] even CTA: the 8 epilogue warps of the pair drained buffer b
 //                (4 local arrivals, 4 remote ones from the odd CTA).
-// A cluster barrier after the MMA and copy drains keeps both CTAs (their
-// shared memory and TMEM) alive until nothing in flight can touch them.  No
-// load uses multicast.
+// Teardown: the odd CTA publishes how many stage loads it issued; after a
+// cluster barrier the even CTA's producer waits for the last load of every
+// stage (both CTAs' copies land on its barriers), first settling the byte
+// count of a stage that only one CTA loaded because the other one aborted
+// (mbarrier.complete_tx for a missing half, an arrive with the expected bytes
+// for a stage the even CTA never armed).  A second cluster barrier then keeps
+// both CTAs (their shared memory and TMEM) alive until no copy or MMA can
+// touch them.  No load uses multicast.
 
 constexpr int kPairStages = 6;
 constexpr int kPairStageBytes = 2 * kABytes;                // 16 KB A half + 16 KB B half
 constexpr uint32_t kIdescPair = (2u << 4) | (1u << 7) | (1u << 10) |
                                 (static_cast<uint32_t>(kTileN >> 3) << 17) |
                                 (static_cast<uint32_t>(256 >> 4) << 24);
+// CRT scratch per CTA and modulus: 16 column chunks x 128 rows x 16 bytes
+constexpr int kCrtChunkBytes = 16 * 128;
+constexpr int kCrtModulusBytes = (kTileN / 16) * kCrtChunkBytes;   // 32 KB
 
 struct __align__(8) PairBarriers {
     uint64_t full[kPairStages];
@@ -522,6 +541,7 @@ struct __align__(8) PairBarriers {
     uint64_t mma_drain;
     uint32_t tmem_base;
     int abort_flag;
+    uint32_t odd_items;   // stage loads issued by the odd CTA (written remotely)
 };
 
 __device__ __forceinline__ uint32_t cluster_ctarank() {
@@ -541,6 +561,15 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
                      cluster_addr)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_complete_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_cluster_u32(uint32_t cluster_addr, uint32_t v) {
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
 }
 
 // TMA load of one 128-row x 128-byte tile (rows y .. y+127 of the workspace
@@ -588,11 +617,176 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
         : "memory");
 }
 
+// One accumulator group: the slice pairs (sa + i, sb - i), i < npairs, over
+// k-tiles [k0, k1).
+struct Group {
+    int sa, sb, npairs, k0, k1, d;
+};
+
+template <bool kCRT>
+__device__ __forceinline__ int n_groups(int ktiles, int nsl, int chunk) {
+    return kCRT ? nsl : nsl * ((ktiles + chunk - 1) / chunk);
+}
+
+// digits: groups run over diagonals d = S-1 .. 0 and, inside, over K chunks;
+// moduli: group m is modulus m over all of K
+template <bool kCRT>
+__device__ __forceinline__ Group group_at(int g, int ktiles, int nsl, int chunk) {
+    Group r;
+    if (kCRT) {
+        r.sa = g;
+        r.sb = g;
+        r.npairs = 1;
+        r.k0 = 0;
+        r.k1 = ktiles;
+        r.d = g;
+    } else {
+        const int nch = (ktiles + chunk - 1) / chunk;
+        r.d = nsl - 1 - g / nch;
+        r.sa = 0;
+        r.sb = r.d;
+        r.npairs = r.d + 1;
+        r.k0 = (g % nch) * chunk;
+        r.k1 = min(ktiles, r.k0 + chunk);
+    }
+    return r;
+}
+
+// 2^k as a double for -1022 <= k <= 1023
+__device__ __forceinline__ double pow2i(int k) {
+    return __hiloint2double((k + 1023) << 20, 0);
+}
+
+// x * 2^k, exact unless the result leaves the normal range (then rounded once,
+// like ldexp)
+__device__ __forceinline__ double scale2(double x, int k) {
+    return (k >= -1022 && k <= 1023) ? x * pow2i(k) : ldexp(x, k);
+}
+
+// the exact double value of a 32-bit signed integer, without the conversion
+// unit: 1.5 * 2^52 + 2^31 + v, minus the constant
+__device__ __forceinline__ double int_to_double(int32_t v) {
+    return __hiloint2double(0x43380000, v ^ static_cast<int32_t>(0x80000000)) -
+           6755401588539392.0;
+}
+
+constexpr double kRoundMagic = 6755399441055744.0;   // 1.5 * 2^52: x + M rounds x to an integer
+
+// symmetric residue of the int32 accumulator acc modulo the odd modulus p,
+// as the low byte of acc - p * rint(acc / p) (the quotient is exact: |acc/p| <
+// 2^24 and acc/p is at least 1/(2p) away from any half integer)
+__device__ __forceinline__ uint32_t residue_byte(int32_t acc, int32_t p, double inv_p) {
+    const int32_t q = __double2loint(fma(int_to_double(acc), inv_p, kRoundMagic));
+    return static_cast<uint32_t>(acc - q * p) & 0xFFu;
+}
+
+// CRT constants of one modulus count (host computed, passed by value): the
+// moduli, 1/p_m rounded, y_m / p_m (y_m = (P/p_m)^-1 mod p_m) as FP32, the CRT
+// weights W_m = (P/p_m) y_m split as w1_m + w2_m + (dropped) on the grids 2^e1
+// and 2^e2, and P split the same way.
+struct CrtConsts {
+    int32_t n, e1, e2, pad;
+    int32_t p[FS_OZAKI2_MAX_MODULI];
+    float f[FS_OZAKI2_MAX_MODULI];
+    double inv_p[FS_OZAKI2_MAX_MODULI];
+    double w1[FS_OZAKI2_MAX_MODULI];
+    double w2[FS_OZAKI2_MAX_MODULI];
+    double p1, p2;
+};
+
+// ------------------------------------------------ Ozaki II (CRT over moduli)
+//
+// The integer-modular form of the Ozaki scheme (Ozaki, Uchino, Imamura,
+// "Ozaki Scheme II: a GEMM-oriented emulation of floating-point matrix
+// multiplication using an integer modular technique", 2025): every row i of
+// op(A) is scaled by 2^(a - e_i) (e_i the frexp exponent of the row maximum)
+// and rounded to an integer A'_ik with |A'_ik| <= 2^a; likewise the columns of
+// op(B) with b bits.  The exact integer product X = A' B' satisfies
+// |X| <= K 2^(a+b) <= P / 4 for P = p_0 ... p_(n-1), the product of n pairwise
+// coprime moduli <= 256, so X is recovered from its residues X mod p_m.  Each
+// residue product is one int8 GEMM of the symmetric residues of A' and B'
+// (entries in [-128, 127], exact int32 accumulation for K < 2^17).  The CRT
+// then gives X = sum_m r_m W_m - k P with W_m = (P/p_m) ((P/p_m)^-1 mod p_m),
+// k = rint(sum_m r_m y_m / p_m), evaluated exactly in FP64 by splitting every
+// W_m (and P) into two doubles on fixed binary grids 2^E1 and 2^E2 so that
+// every product and partial sum is representable; the dropped remainder is
+// below 2^(E2 + 12), far under the rounding of A and B.  C = alpha X 2^(e_i +
+// f_j - a - b) + beta C.  One int8 product per modulus replaces the
+// S(S+1)/2 digit-slice products of the Ozaki I form.
+
+constexpr int kCrtMaxModuli = FS_OZAKI2_MAX_MODULI;
+
+// the moduli, largest first; pairwise coprime (256 = 2^8, 255 = 3*5*17,
+// 253 = 11*23, 247 = 13*19, 217 = 7*31, the rest prime)
+constexpr int32_t kModuli[kCrtMaxModuli] = {256, 255, 253, 251, 247, 241, 239,
+                                            233, 229, 227, 223, 217, 211, 199};
+
+template <class Prob>
+__device__ __forceinline__ void crt_store_row(const Prob& p, const CrtConsts& cc,
+                                              const uint8_t* scratch, int64_t row, int col0,
+                                              int ea) {
+    const int n = cc.n;
+    double* crow = p.C + row * p.ldc;
+    const int sa = ea - p.a_bits - p.b_bits;
+    for (int cb = 0; cb < kTileN && col0 + cb < p.N; cb += 16) {
+        uint32_t w[kCrtMaxModuli][4];
+#pragma unroll
+        for (int m = 0; m < kCrtMaxModuli; ++m) {
+            if (m < n) {
+                const uint4 q = *reinterpret_cast<const uint4*>(
+                    scratch + m * kCrtModulusBytes + (cb / 16) * kCrtChunkBytes);
+                w[m][0] = q.x;
+                w[m][1] = q.y;
+                w[m][2] = q.z;
+                w[m][3] = q.w;
+            }
+        }
+        const int ncol = min(16, p.N - col0 - cb);
+        const int32_t* be = p.b_exps + col0 + cb;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j < ncol) {
+                // k = rint(sum_m r_m y_m / p_m) in FP32: |sum| < 2^12 and the
+                // rounding errors stay below 1/100, while the fractional part
+                // X / P is within 1/4 of an integer
+                float kf = 0.0f;
+#pragma unroll
+                for (int m = 0; m < kCrtMaxModuli; ++m) {
+                    if (m < n) {
+                        const int32_t r =
+                            static_cast<int32_t>(static_cast<int8_t>(w[m][j / 4] >> (8 * (j % 4))));
+                        kf = fmaf(__int_as_float(0x4B400000 + r) - 12582912.0f, cc.f[m], kf);
+                    }
+                }
+                const int32_t k = __float_as_int(kf + 12582912.0f) - 0x4B400000;
+                const double kd = int_to_double(k);
+                double d1 = -kd * cc.p1;
+                double d2 = -kd * cc.p2;
+#pragma unroll
+                for (int m = 0; m < kCrtMaxModuli; ++m) {
+                    if (m < n) {
+                        const int32_t r =
+                            static_cast<int32_t>(static_cast<int8_t>(w[m][j / 4] >> (8 * (j % 4))));
+                        const double rd = int_to_double(r);
+                        d1 = fma(rd, cc.w1[m], d1);
+                        d2 = fma(rd, cc.w2[m], d2);
+                    }
+                }
+                const double x = d1 + d2;
+                const double val = p.alpha * scale2(x, sa + __ldg(be + j));
+                double* dst = crow + col0 + cb + j;
+                *dst = (p.beta == 0.0) ? val : fma(p.beta, *dst, val);
+            }
+        }
+    }
+}
+
+template <class Prob, bool kCRT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-    k_oz_gemm_pair(const FsOzProblem* __restrict__ probs, int64_t n_probs,
-                   const FsOzTile* __restrict__ tiles, int64_t n_tiles, int nslices,
-                   int chunk_ktiles, int32_t* flag, const __grid_constant__ CUtensorMap ws_map,
-                   const int8_t* ws_base, long long spin) {
+    k_oz_pair(const Prob* __restrict__ probs, int64_t n_probs, const FsOzTile* __restrict__ tiles,
+              int64_t n_tiles, int nslices, int chunk_ktiles, int32_t* flag,
+              const __grid_constant__ CUtensorMap ws_map, const int8_t* ws_base, long long spin,
+              uint8_t* crt_scratch, const __grid_constant__ CrtConsts cc) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -614,6 +808,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         }
         mbar_init(smem_addr(&bars->mma_drain), 1);
         bars->abort_flag = 0;
+        bars->odd_items = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -629,6 +824,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem_base = bars->tmem_base;
     volatile int* abort_flag = &bars->abort_flag;
+    uint32_t items = 0;   // stage loads issued by this CTA's producer
 
     if (warp == 0) {
         // ------------------------------------------ producer (both CTAs)
@@ -636,55 +832,48 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             int stage = 0;
             uint32_t phase = 0;
             bool ok = true;
-            uint32_t issued_mask = 0, issued_parity = 0;
             for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
                 const FsOzTile tile = tiles[t];
-                const FsOzProblem p = probs[tile.problem];
+                const Prob p = probs[tile.problem];
+                if (kCRT && p.K > FS_OZAKI2_MAX_K) continue;
                 const int64_t a_slice = static_cast<int64_t>(p.ktiles) * p.a_rowtiles * kABytes;
                 const int64_t b_slice = static_cast<int64_t>(p.ktiles) * p.b_rowtiles * kABytes;
                 const int a_rt = 2 * tile.tm + static_cast<int>(rank);
                 const int b_rt = 2 * tile.tn + static_cast<int>(rank);
-                for (int d = nslices - 1; ok && d >= 0; --d) {
-                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
-                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
-                        for (int s = 0; ok && s <= d; ++s) {
-                            for (int kt = k0; kt < k1; ++kt) {
-                                if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1,
-                                               abort_flag, spin)) {
-                                    ok = false;
-                                    break;
-                                }
-                                const uint32_t full = smem_addr(&bars->full[stage]);
-                                if (rank == 0) mbar_expect_tx(full, 2 * kPairStageBytes);
-                                const int8_t* a = p.a_slices + s * a_slice +
-                                                  (static_cast<int64_t>(kt) * p.a_rowtiles + a_rt) * kABytes;
-                                const int8_t* b = p.b_slices + (d - s) * b_slice +
-                                                  (static_cast<int64_t>(kt) * p.b_rowtiles + b_rt) * kABytes;
-                                const uint32_t dst = base + stage * kPairStageBytes;
-                                const uint32_t full_even = map_to_rank(full, 0);
-                                tma_tile_pair(dst, &ws_map, static_cast<int32_t>((a - ws_base) >> 7),
-                                              full_even);
-                                tma_tile_pair(dst + kABytes, &ws_map,
-                                              static_cast<int32_t>((b - ws_base) >> 7), full_even);
-                                issued_mask |= 1u << stage;
-                                issued_parity = (issued_parity & ~(1u << stage)) | (phase << stage);
-                                if (++stage == kPairStages) {
-                                    stage = 0;
-                                    phase ^= 1;
-                                }
+                const int ng = n_groups<kCRT>(p.ktiles, nslices, chunk_ktiles);
+                for (int g = 0; ok && g < ng; ++g) {
+                    const Group gr = group_at<kCRT>(g, p.ktiles, nslices, chunk_ktiles);
+                    for (int i = 0; ok && i < gr.npairs; ++i) {
+                        const int8_t* a_sl = p.a_slices + (gr.sa + i) * a_slice;
+                        const int8_t* b_sl = p.b_slices + (gr.sb - i) * b_slice;
+                        for (int kt = gr.k0; kt < gr.k1; ++kt) {
+                            if (!mbar_wait(smem_addr(&bars->empty[stage]), phase ^ 1, abort_flag,
+                                           spin)) {
+                                ok = false;
+                                break;
+                            }
+                            const uint32_t full = smem_addr(&bars->full[stage]);
+                            if (rank == 0) mbar_expect_tx(full, 2 * kPairStageBytes);
+                            const int8_t* a =
+                                a_sl + (static_cast<int64_t>(kt) * p.a_rowtiles + a_rt) * kABytes;
+                            const int8_t* b =
+                                b_sl + (static_cast<int64_t>(kt) * p.b_rowtiles + b_rt) * kABytes;
+                            const uint32_t dst = base + stage * kPairStageBytes;
+                            const uint32_t full_even = map_to_rank(full, 0);
+                            tma_tile_pair(dst, &ws_map, static_cast<int32_t>((a - ws_base) >> 7),
+                                          full_even);
+                            tma_tile_pair(dst + kABytes, &ws_map,
+                                          static_cast<int32_t>((b - ws_base) >> 7), full_even);
+                            ++items;
+                            if (++stage == kPairStages) {
+                                stage = 0;
+                                phase ^= 1;
                             }
                         }
                     }
                 }
             }
-            // the even CTA's full barriers complete only when the copies of
-            // both CTAs have landed
-            for (int s = 0; rank == 0 && s < kPairStages; ++s) {
-                if (issued_mask & (1u << s)) {
-                    if (!mbar_wait_drain(smem_addr(&bars->full[s]), (issued_parity >> s) & 1u))
-                        *abort_flag = 1;
-                }
-            }
+            if (rank == 1) st_cluster_u32(map_to_rank(smem_addr(&bars->odd_items), 0), items);
         }
     } else if (warp == 1 && rank == 1) {
         // the odd CTA's warp 1 only shares the TMEM allocation
@@ -697,46 +886,47 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             uint32_t acc_phase = 0;
             bool ok = true;
             for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
-                const FsOzProblem p = probs[tiles[t].problem];
-                for (int d = nslices - 1; ok && d >= 0; --d) {
-                    for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
-                        const int k1 = min(p.ktiles, k0 + chunk_ktiles);
-                        if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1,
-                                       abort_flag, spin)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const uint32_t tmem_d = tmem_base + acc * kTileN;
-                        uint32_t accumulate = 0;
-                        for (int s = 0; ok && s <= d; ++s) {
-                            for (int kt = k0; kt < k1; ++kt) {
-                                if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag, spin)) {
-                                    ok = false;
-                                    break;
-                                }
-                                tc_fence_after();
-                                const uint32_t a_addr = base + stage * kPairStageBytes;
-                                const uint32_t b_addr = a_addr + kABytes;
+                const Prob p = probs[tiles[t].problem];
+                if (kCRT && p.K > FS_OZAKI2_MAX_K) continue;
+                const int ng = n_groups<kCRT>(p.ktiles, nslices, chunk_ktiles);
+                for (int g = 0; ok && g < ng; ++g) {
+                    const Group gr = group_at<kCRT>(g, p.ktiles, nslices, chunk_ktiles);
+                    if (!mbar_wait(smem_addr(&bars->acc_empty[acc]), acc_phase ^ 1, abort_flag,
+                                   spin)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t tmem_d = tmem_base + acc * kTileN;
+                    uint32_t accumulate = 0;
+                    for (int i = 0; ok && i < gr.npairs; ++i) {
+                        for (int kt = gr.k0; kt < gr.k1; ++kt) {
+                            if (!mbar_wait(smem_addr(&bars->full[stage]), phase, abort_flag,
+                                           spin)) {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint32_t a_addr = base + stage * kPairStageBytes;
+                            const uint32_t b_addr = a_addr + kABytes;
 #pragma unroll
-                                for (int k = 0; k < kTileK / 32; ++k) {
-                                    mma_i8_pair(tmem_d, smem_desc_sw128(a_addr + 32 * k),
-                                                smem_desc_sw128(b_addr + 32 * k), accumulate);
-                                    accumulate = 1;
-                                }
-                                mma_commit_pair(smem_addr(&bars->empty[stage]));
-                                if (++stage == kPairStages) {
-                                    stage = 0;
-                                    phase ^= 1;
-                                }
+                            for (int k = 0; k < kTileK / 32; ++k) {
+                                mma_i8_pair(tmem_d, smem_desc_sw128(a_addr + 32 * k),
+                                            smem_desc_sw128(b_addr + 32 * k), accumulate);
+                                accumulate = 1;
+                            }
+                            mma_commit_pair(smem_addr(&bars->empty[stage]));
+                            if (++stage == kPairStages) {
+                                stage = 0;
+                                phase ^= 1;
                             }
                         }
-                        if (!ok) break;
-                        mma_commit_pair(smem_addr(&bars->acc_full[acc]));
-                        if (++acc == 2) {
-                            acc = 0;
-                            acc_phase ^= 1;
-                        }
+                    }
+                    if (!ok) break;
+                    mma_commit_pair(smem_addr(&bars->acc_full[acc]));
+                    if (++acc == 2) {
+                        acc = 0;
+                        acc_phase ^= 1;
                     }
                 }
             }
@@ -746,37 +936,71 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     } else {
         // ------------------------------------------ epilogue (both CTAs)
         const int quad = warp % 4;
-        const int row_in_tile = static_cast<int>(rank) * 128 + quad * 32 + lane;
+        const int lrow = quad * 32 + lane;                // TMEM lane = row within this CTA
+        const int row_in_tile = static_cast<int>(rank) * 128 + lrow;
         const uint32_t acc_empty_leader[2] = {
             map_to_rank(smem_addr(&bars->acc_empty[0]), 0),
             map_to_rank(smem_addr(&bars->acc_empty[1]), 0)};
+        uint8_t* my_scratch = nullptr;
+        if (kCRT)
+            my_scratch = crt_scratch + static_cast<int64_t>(blockIdx.x) * nslices * kCrtModulusBytes +
+                         lrow * 16;
         int acc = 0;
         uint32_t acc_phase = 0;
         bool ok = true;
         for (int64_t t = cluster_id; ok && t < n_tiles; t += n_clusters) {
             const FsOzTile tile = tiles[t];
-            const FsOzProblem p = probs[tile.problem];
+            const Prob p = probs[tile.problem];
+            if (kCRT && p.K > FS_OZAKI2_MAX_K) {
+                // the int32 residue products could overflow: skipped, reported
+                if (threadIdx.x == 64) raise_flag(flag, FS_ERR_UNSUPPORTED);
+                continue;
+            }
             const int64_t row = static_cast<int64_t>(tile.tm) * 256 + row_in_tile;
             const int col0 = tile.tn * kTileN;
             const bool row_ok = row < p.M;
             const int ea = row_ok ? p.a_exps[row] : 0;
+            const int ng = n_groups<kCRT>(p.ktiles, nslices, chunk_ktiles);
             bool first = true;
-            for (int d = nslices - 1; ok && d >= 0; --d) {
-                for (int k0 = 0; ok && k0 < p.ktiles; k0 += chunk_ktiles) {
-                    int got = 0;
-                    if (lane == 0)
-                        got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag, spin)
-                                  ? 1
-                                  : 0;
-                    got = __shfl_sync(0xffffffffu, got, 0);
-                    if (!got) {
-                        ok = false;
-                        break;
+            for (int g = 0; ok && g < ng; ++g) {
+                int got = 0;
+                if (lane == 0)
+                    got = mbar_wait(smem_addr(&bars->acc_full[acc]), acc_phase, abort_flag, spin)
+                              ? 1
+                              : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t taddr =
+                    tmem_base + (static_cast<uint32_t>(quad * 32) << 16) + acc * kTileN;
+                if constexpr (kCRT) {
+                    // residues of modulus g, one byte per entry, parked in this
+                    // thread's slots of the CTA scratch
+                    const int32_t pm = cc.p[g];
+                    const double ipm = cc.inv_p[g];
+                    uint8_t* dst = my_scratch + static_cast<int64_t>(g) * kCrtModulusBytes;
+                    for (int cb = 0; cb < kTileN; cb += 16) {
+                        uint32_t v[16];
+                        tmem_ld16(taddr + cb, v);
+                        uint32_t w[4] = {0, 0, 0, 0};
+                        if (g == 0) {
+                            // p = 256: the low byte is the symmetric residue
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) w[j / 4] |= (v[j] & 0xFFu) << (8 * (j % 4));
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                w[j / 4] |= residue_byte(static_cast<int32_t>(v[j]), pm, ipm)
+                                            << (8 * (j % 4));
+                        }
+                        *reinterpret_cast<uint4*>(dst + (cb / 16) * kCrtChunkBytes) =
+                            make_uint4(w[0], w[1], w[2], w[3]);
                     }
-                    tc_fence_after();
-                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quad * 32) << 16) +
-                                           acc * kTileN;
-                    const int shift = -7 * (d + 2);
+                } else {
+                    const int shift = -7 * (group_at<kCRT>(g, p.ktiles, nslices, chunk_ktiles).d + 2);
                     const bool read_c = !first || p.beta != 0.0;
                     for (int cb = 0; cb < kTileN; cb += 16) {
                         uint32_t v[16];
@@ -804,32 +1028,171 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         for (int j = 0; j < 16; ++j)
                             if (j < ncol) crow[j] = old[j];
                     }
-                    first = false;
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) {
-                        if (rank == 0)
-                            mbar_arrive(smem_addr(&bars->acc_empty[acc]));
-                        else
-                            mbar_arrive_remote(acc_empty_leader[acc]);
-                    }
-                    if (++acc == 2) {
-                        acc = 0;
-                        acc_phase ^= 1;
-                    }
+                }
+                first = false;
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    if (rank == 0)
+                        mbar_arrive(smem_addr(&bars->acc_empty[acc]));
+                    else
+                        mbar_arrive_remote(acc_empty_leader[acc]);
+                }
+                if (++acc == 2) {
+                    acc = 0;
+                    acc_phase ^= 1;
+                }
+                if constexpr (kCRT) {
+                    if (g == ng - 1 && row_ok) crt_store_row(p, cc, my_scratch, row, col0, ea);
                 }
             }
         }
     }
 
     __syncthreads();
-    cluster_sync_all();  // no MMA of the pair can touch either CTA after this
+    cluster_sync_all();  // every role done; the odd CTA's load count is visible
+    if (rank == 0 && threadIdx.x == 0) {
+        // wait for the last load of every stage, settling stages that only one
+        // CTA loaded (see the teardown note above)
+        const uint32_t n_odd = bars->odd_items;
+        const uint32_t n_even = items;
+        const uint32_t n_max = n_even > n_odd ? n_even : n_odd;
+        const uint32_t first = n_max > static_cast<uint32_t>(kPairStages) ? n_max - kPairStages : 0;
+        for (uint32_t i = first; i < n_max; ++i) {
+            const uint32_t bar = smem_addr(&bars->full[i % kPairStages]);
+            if (i >= n_even)
+                mbar_expect_tx(bar, kPairStageBytes);
+            else if (i >= n_odd)
+                mbar_complete_tx(bar, kPairStageBytes);
+            if (!mbar_wait_drain(bar, (i / kPairStages) & 1u)) *abort_flag = 1;
+        }
+    }
+    __syncthreads();
+    cluster_sync_all();  // no copy or MMA of the pair can touch either CTA after this
     if (threadIdx.x == 0 && *abort_flag) raise_flag(flag, FS_ERR_TIMEOUT);
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                      "r"(kTmemCols)
                      : "memory");
+    }
+}
+
+// Residue slices of one Ozaki II operand: for every entry, A' = rint(x 2^(bits
+// - e_row)) (|A'| <= 2^bits <= 2^50) and its symmetric residues modulo the n
+// moduli, one int8 slice per modulus in the swizzled tile layout of the digit
+// slices.  A' stays exact in FP64; adding 1.5 * 2^52 rounds to the integer and
+// leaves A' mod 2^32 in the low word.  For an odd modulus p the quotient
+// q = rint(A' / p) comes from one FMA (|A' / p| < 2^43, so the rounded 1/p
+// moves A'/p by less than 2^-10, while A'/p lies at least 1/(2p) > 2^-9 from
+// any half integer) and the residue is the low byte of A' - q p computed in
+// 32-bit integers.  For p = 256 it is the low byte of A'.
+//
+// Thread mapping: a block handles a 32-row group of one k-tile (32 rows x 128
+// k values); each thread 16 consecutive k of one row.  When the operand's rows
+// are contiguous in memory (transposed storage) a warp spans 32 rows at one
+// k-chunk, otherwise 4 rows x 8 chunks, so both layouts read coalesced.
+__global__ void __launch_bounds__(256)
+    k_oz2_split(const FsOz2Operand* __restrict__ ops, int64_t n_ops,
+                const __grid_constant__ CrtConsts cc) {
+    const int op_id = blockIdx.y;
+    if (op_id >= n_ops) return;
+    const FsOz2Operand op = ops[op_id];
+    const bool rows_contiguous = (op.s_row == 1 && op.s_k != 1);
+    const int t = threadIdx.x;
+    const int r = rows_contiguous ? (t & 31) : (t >> 3);   // row within the 32-row group
+    const int c = rows_contiguous ? (t >> 5) : (t & 7);    // 16-byte chunk of the k-tile
+    const int groups = op.rowtiles * (kSplitRows / 32);
+    const int64_t units = static_cast<int64_t>(groups) * op.ktiles;
+    const int64_t slice_stride = static_cast<int64_t>(op.ktiles) * op.rowtiles * kABytes;
+    const int n = cc.n;
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int kt = static_cast<int>(u / groups);
+        const int rg = static_cast<int>(u % groups);
+        const int rt = rg / (kSplitRows / 32);
+        const int rr = (rg % (kSplitRows / 32)) * 32 + r;       // row within the tile
+        const int64_t row = static_cast<int64_t>(rt) * kSplitRows + rr;
+        const int64_t k0 = static_cast<int64_t>(kt) * kTileK + c * 16;
+        const bool row_ok = row < op.rows;
+        const int sh = op.bits - (row_ok ? op.exps[row] : 0);
+        int32_t lo[16];
+        double ad[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int64_t k = k0 + j;
+            const double x =
+                (row_ok && k < op.K) ? __ldg(op.src + row * op.s_row + k * op.s_k) : 0.0;
+            const double tt = scale2(x, sh) + kRoundMagic;
+            lo[j] = __double2loint(tt);
+            ad[j] = tt - kRoundMagic;
+        }
+        int8_t* dst = op.slices + (static_cast<int64_t>(kt) * op.rowtiles + rt) * kABytes +
+                      rr * 128 + ((c ^ (rr & 7)) * 16);
+        {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                w[j / 4] |= (static_cast<uint32_t>(lo[j]) & 0xFFu) << (8 * (j % 4));
+            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        for (int m = 1; m < n; ++m) {
+            const int32_t pm = cc.p[m];
+            const double ipm = cc.inv_p[m];
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int32_t q = __double2loint(fma(ad[j], ipm, kRoundMagic));
+                w[j / 4] |= (static_cast<uint32_t>(lo[j] - q * pm) & 0xFFu) << (8 * (j % 4));
+            }
+            *reinterpret_cast<uint4*>(dst + m * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+// Row exponents of Ozaki II operands (exps[v] = e with max_k |x(v, k)| < 2^e,
+// 0 for a zero row): one warp per row when k is contiguous, else a 32-row x
+// 8-lane block per row group so that a warp reads 32 consecutive rows.
+__global__ void __launch_bounds__(256)
+    k_oz2_exponents(const FsOz2Operand* __restrict__ ops, int64_t n_ops) {
+    const int op_id = blockIdx.y;
+    if (op_id >= n_ops) return;
+    const FsOz2Operand op = ops[op_id];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (!(op.s_row == 1 && op.s_k != 1)) {
+        for (int64_t v = static_cast<int64_t>(blockIdx.x) * 8 + warp; v < op.rows;
+             v += static_cast<int64_t>(gridDim.x) * 8) {
+            double m = 0.0;
+            for (int64_t k = lane; k < op.K; k += 32)
+                m = fmax(m, fabs(__ldg(op.src + v * op.s_row + k * op.s_k)));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) {
+                int e = 0;
+                if (m > 0.0) frexp(m, &e);
+                op.exps[v] = e;
+            }
+        }
+        return;
+    }
+    __shared__ double part[8][33];
+    for (int64_t v0 = static_cast<int64_t>(blockIdx.x) * 32; v0 < op.rows;
+         v0 += static_cast<int64_t>(gridDim.x) * 32) {
+        const int64_t v = v0 + lane;
+        double m = 0.0;
+        if (v < op.rows)
+            for (int64_t k = warp; k < op.K; k += 8) m = fmax(m, fabs(__ldg(op.src + v + k * op.s_k)));
+        part[warp][lane] = m;
+        __syncthreads();
+        if (warp == 0) {
+#pragma unroll
+            for (int w = 1; w < 8; ++w) m = fmax(m, part[w][lane]);
+            if (v < op.rows) {
+                int e = 0;
+                if (m > 0.0) frexp(m, &e);
+                op.exps[v] = e;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -910,6 +1273,198 @@ EncodeTiledFn encode_tiled() {
 
 }  // namespace
 
+// ------------------------------------------------- Ozaki II host side
+
+namespace {
+
+using u128 = unsigned __int128;
+
+int bitlen(u128 x) {
+    int b = 0;
+    while (x != 0) {
+        ++b;
+        x >>= 1;
+    }
+    return b;
+}
+
+// CRT constants for the first n moduli (exact integer arithmetic: P < 2^111)
+bool make_crt_consts(int n, fsb::oz::CrtConsts* c) {
+    using fsb::oz::kModuli;
+    if (n < FS_OZAKI2_MIN_MODULI || n > FS_OZAKI2_MAX_MODULI) return false;
+    std::memset(c, 0, sizeof(*c));
+    u128 P = 1;
+    for (int m = 0; m < n; ++m) P *= static_cast<u128>(kModuli[m]);
+    // |sum_m r_m W_m| + |k| P <= 128 n P + 128 n P
+    const u128 bound = P * static_cast<u128>(256 * n);
+    int e1 = bitlen(bound) - 53;
+    if (e1 < 0) e1 = 0;
+    int e2 = e1 + bitlen(static_cast<u128>(256 * n)) - 53;
+    if (e2 < 0) e2 = 0;
+    c->n = n;
+    c->e1 = e1;
+    c->e2 = e2;
+    for (int m = 0; m < n; ++m) {
+        const int32_t p = kModuli[m];
+        const u128 Q = P / static_cast<u128>(p);
+        const int32_t qm = static_cast<int32_t>(Q % static_cast<u128>(p));
+        int32_t y = 0;
+        for (int32_t t = 1; t < p; ++t)
+            if ((static_cast<int64_t>(qm) * t) % p == 1) {
+                y = t;
+                break;
+            }
+        if (y == 0) return false;
+        const u128 W = Q * static_cast<u128>(y);
+        const u128 w1 = (W >> e1) << e1;
+        c->p[m] = p;
+        c->inv_p[m] = 1.0 / static_cast<double>(p);
+        c->f[m] = static_cast<float>(static_cast<double>(y) / static_cast<double>(p));
+        c->w1[m] = std::ldexp(static_cast<double>(static_cast<uint64_t>(W >> e1)), e1);
+        c->w2[m] = std::ldexp(static_cast<double>(static_cast<uint64_t>((W - w1) >> e2)), e2);
+    }
+    const u128 p1 = (P >> e1) << e1;
+    c->p1 = std::ldexp(static_cast<double>(static_cast<uint64_t>(P >> e1)), e1);
+    c->p2 = std::ldexp(static_cast<double>(static_cast<uint64_t>((P - p1) >> e2)), e2);
+    return true;
+}
+
+const fsb::oz::CrtConsts* crt_consts(int n) {
+    static fsb::oz::CrtConsts table[FS_OZAKI2_MAX_MODULI + 1];
+    static bool ok[FS_OZAKI2_MAX_MODULI + 1];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (int k = FS_OZAKI2_MIN_MODULI; k <= FS_OZAKI2_MAX_MODULI; ++k)
+            ok[k] = make_crt_consts(k, &table[k]);
+    });
+    if (n < FS_OZAKI2_MIN_MODULI || n > FS_OZAKI2_MAX_MODULI || !ok[n]) return nullptr;
+    return &table[n];
+}
+
+// tensor map viewing a workspace as rows of 128 bytes (box 128 x 128): a
+// 16-byte aligned base, whole rows, and row indices that fit the 32-bit TMA
+// coordinate
+int workspace_map(const void* d_workspace, int64_t workspace_bytes, CUtensorMap* map) {
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 127u) != 0 || workspace_bytes < 128 * 128 ||
+        (workspace_bytes & 127) != 0 || (workspace_bytes >> 7) >= (1LL << 31))
+        return FS_ERR_INVALID_ARG;
+    EncodeTiledFn enc = encode_tiled();
+    if (enc == nullptr) return FS_ERR_UNSUPPORTED;
+    const cuuint64_t dims[2] = {128, static_cast<cuuint64_t>(workspace_bytes >> 7)};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {128, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(d_workspace), dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return FS_ERR_INVALID_ARG;
+    return FS_OK;
+}
+
+constexpr int kPairSmem = fsb::oz::kPairStages * fsb::oz::kPairStageBytes +
+                          static_cast<int>(sizeof(fsb::oz::PairBarriers)) + 1024;
+
+}  // namespace
+
+extern "C" int fs_ozaki2_bits(int32_t nmod, int64_t K, int32_t* a_bits, int32_t* b_bits) {
+    if (a_bits == nullptr || b_bits == nullptr || K < 0) return FS_ERR_INVALID_ARG;
+    if (nmod < FS_OZAKI2_MIN_MODULI || nmod > FS_OZAKI2_MAX_MODULI) return FS_ERR_INVALID_ARG;
+    if (K > FS_OZAKI2_MAX_K) return FS_ERR_UNSUPPORTED;
+    u128 P = 1;
+    for (int m = 0; m < nmod; ++m) P *= static_cast<u128>(fsb::oz::kModuli[m]);
+    int ck = 0;
+    while ((int64_t{1} << ck) < (K > 1 ? K : 1)) ++ck;
+    // |X| <= K 2^(a+b) <= P / 4
+    const int L = (bitlen(P) - 1) - 2 - ck;
+    int a = L / 2;
+    int b = L - a;
+    if (a > 50) a = 50;
+    if (b > 50) b = 50;
+    if (a < 1) return FS_ERR_UNSUPPORTED;
+    *a_bits = a;
+    *b_bits = b;
+    return FS_OK;
+}
+
+extern "C" int fs_ozaki2_constants(int32_t nmod, int32_t* moduli, double* weights_hi,
+                                   double* weights_lo, double* modulus_product, float* frac,
+                                   int32_t* grids) {
+    const fsb::oz::CrtConsts* c = crt_consts(nmod);
+    if (c == nullptr) return FS_ERR_INVALID_ARG;
+    if (!moduli || !weights_hi || !weights_lo || !modulus_product || !frac || !grids)
+        return FS_ERR_INVALID_ARG;
+    for (int m = 0; m < nmod; ++m) {
+        moduli[m] = c->p[m];
+        weights_hi[m] = c->w1[m];
+        weights_lo[m] = c->w2[m];
+        frac[m] = c->f[m];
+    }
+    modulus_product[0] = c->p1;
+    modulus_product[1] = c->p2;
+    grids[0] = c->e1;
+    grids[1] = c->e2;
+    return FS_OK;
+}
+
+extern "C" int fs_ozaki2_scratch_bytes(int32_t nmod, int64_t* bytes) {
+    if (bytes == nullptr) return FS_ERR_INVALID_ARG;
+    if (nmod < FS_OZAKI2_MIN_MODULI || nmod > FS_OZAKI2_MAX_MODULI) return FS_ERR_INVALID_ARG;
+    const int64_t ctas = 2 * (fsb::num_sms() / 2);
+    *bytes = ctas * nmod * static_cast<int64_t>(fsb::oz::kCrtModulusBytes);
+    return FS_OK;
+}
+
+extern "C" int fs_ozaki2_split(const FsOz2Operand* d_ops, int64_t n_ops, int32_t max_rows,
+                               int64_t max_units, int32_t nmod, void* stream) {
+    if (n_ops < 0 || max_rows < 0 || max_units < 0) return FS_ERR_INVALID_ARG;
+    const fsb::oz::CrtConsts* c = crt_consts(nmod);
+    if (c == nullptr) return FS_ERR_INVALID_ARG;
+    if (n_ops == 0 || max_units == 0) return FS_OK;
+    if (d_ops == nullptr) return FS_ERR_INVALID_ARG;
+    if (n_ops > 65535) return FS_ERR_TOO_LARGE;
+    cudaStream_t s = fsb::as_stream(stream);
+    const int sms = fsb::num_sms();
+    const int64_t ge = std::min<int64_t>((max_rows + 7) / 8, 4 * sms);
+    fsb::oz::k_oz2_exponents<<<dim3(static_cast<unsigned>(ge > 0 ? ge : 1),
+                                    static_cast<unsigned>(n_ops)),
+                               256, 0, s>>>(d_ops, n_ops);
+    int st = fsb::launch_status();
+    if (st != FS_OK) return st;
+    const int64_t gs = std::min<int64_t>(max_units, 8 * sms);
+    fsb::oz::k_oz2_split<<<dim3(static_cast<unsigned>(gs), static_cast<unsigned>(n_ops)), 256, 0,
+                           s>>>(d_ops, n_ops, *c);
+    return fsb::launch_status();
+}
+
+extern "C" int fs_ozaki2_gemm_pair(const FsOz2Problem* d_probs, int64_t n_probs,
+                                   const FsOzTile* d_tiles, int64_t n_tiles, int32_t nmod,
+                                   const void* d_workspace, int64_t workspace_bytes,
+                                   void* d_scratch, int64_t scratch_bytes, int32_t* d_flag,
+                                   void* stream) {
+    if (n_probs < 0 || n_tiles < 0) return FS_ERR_INVALID_ARG;
+    const fsb::oz::CrtConsts* c = crt_consts(nmod);
+    if (c == nullptr) return FS_ERR_INVALID_ARG;
+    if (n_tiles == 0) return FS_OK;
+    if (d_probs == nullptr || d_tiles == nullptr || d_workspace == nullptr || d_scratch == nullptr)
+        return FS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_scratch) & 15u) != 0) return FS_ERR_INVALID_ARG;
+    CUtensorMap map;
+    int st = workspace_map(d_workspace, workspace_bytes, &map);
+    if (st != FS_OK) return st;
+    const int64_t max_clusters = fsb::num_sms() / 2;
+    const int clusters = static_cast<int>(n_tiles < max_clusters ? n_tiles : max_clusters);
+    if (scratch_bytes < 2LL * clusters * nmod * fsb::oz::kCrtModulusBytes) return FS_ERR_INVALID_ARG;
+    const void* fn = reinterpret_cast<const void*>(fsb::oz::k_oz_pair<FsOz2Problem, true>);
+    st = fsb::configure_smem(fn, kPairSmem);
+    if (st != FS_OK) return st;
+    fsb::oz::k_oz_pair<FsOz2Problem, true>
+        <<<2 * clusters, fsb::oz::kThreads, kPairSmem, fsb::as_stream(stream)>>>(
+            d_probs, n_probs, d_tiles, n_tiles, nmod, 1, d_flag, map,
+            static_cast<const int8_t*>(d_workspace), fsb::spin_limit(),
+            static_cast<uint8_t*>(d_scratch), *c);
+    return fsb::launch_status();
+}
+
 extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
                                   const FsOzTile* d_tiles, int64_t n_tiles, int32_t nslices,
                                   int32_t chunk_ktiles, const void* d_workspace,
@@ -919,35 +1474,23 @@ extern "C" int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
     if (n_tiles == 0) return FS_OK;
     if (d_probs == nullptr || d_tiles == nullptr || d_workspace == nullptr)
         return FS_ERR_INVALID_ARG;
-    // the workspace is viewed as rows of 128 bytes: 16-byte aligned base, whole
-    // rows, and row indices that fit the 32-bit TMA coordinate
-    if ((reinterpret_cast<uintptr_t>(d_workspace) & 127u) != 0 || workspace_bytes < 128 * 128 ||
-        (workspace_bytes & 127) != 0 || (workspace_bytes >> 7) >= (1LL << 31))
-        return FS_ERR_INVALID_ARG;
-    EncodeTiledFn enc = encode_tiled();
-    if (enc == nullptr) return FS_ERR_UNSUPPORTED;
     CUtensorMap map;
-    const cuuint64_t dims[2] = {128, static_cast<cuuint64_t>(workspace_bytes >> 7)};
-    const cuuint64_t strides[1] = {128};
-    const cuuint32_t box[2] = {128, 128};
-    const cuuint32_t estr[2] = {1, 1};
-    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(d_workspace), dims, strides,
-            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return FS_ERR_INVALID_ARG;
+    int st = workspace_map(d_workspace, workspace_bytes, &map);
+    if (st != FS_OK) return st;
     const long long bound = static_cast<long long>(nslices) * chunk_ktiles * fsb::oz::kTileK *
                             127LL * 127LL;
     if (bound >= (1LL << 31)) return FS_ERR_INVALID_ARG;
-    const int smem = fsb::oz::kPairStages * fsb::oz::kPairStageBytes +
-                     static_cast<int>(sizeof(fsb::oz::PairBarriers)) + 1024;
-    const int cfg =
-        fsb::configure_smem(reinterpret_cast<const void*>(fsb::oz::k_oz_gemm_pair), smem);
-    if (cfg != FS_OK) return cfg;
+    const void* fn = reinterpret_cast<const void*>(fsb::oz::k_oz_pair<FsOzProblem, false>);
+    st = fsb::configure_smem(fn, kPairSmem);
+    if (st != FS_OK) return st;
     const int64_t max_clusters = fsb::num_sms() / 2;
     const int clusters = static_cast<int>(n_tiles < max_clusters ? n_tiles : max_clusters);
-    fsb::oz::k_oz_gemm_pair<<<2 * clusters, fsb::oz::kThreads, smem, fsb::as_stream(stream)>>>(
-        d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag, map,
-        static_cast<const int8_t*>(d_workspace), fsb::spin_limit());
+    fsb::oz::CrtConsts unused;
+    std::memset(&unused, 0, sizeof(unused));
+    fsb::oz::k_oz_pair<FsOzProblem, false>
+        <<<2 * clusters, fsb::oz::kThreads, kPairSmem, fsb::as_stream(stream)>>>(
+            d_probs, n_probs, d_tiles, n_tiles, nslices, chunk_ktiles, d_flag, map,
+            static_cast<const int8_t*>(d_workspace), fsb::spin_limit(), nullptr, unused);
     return fsb::launch_status();
 }
 

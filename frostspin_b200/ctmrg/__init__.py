@@ -1,4 +1,6 @@
 from .classical_c4v import (
+    correlation_length,
+    edge_transfer_spectrum,
     energy_per_bond,
     env_1site,
     env_2sites,
@@ -16,6 +18,8 @@ __all__ = [
     "SequentialCTMRG",
     "SimultaneousCTMRG",
     "SymmetrizedCTMRG",
+    "correlation_length",
+    "edge_transfer_spectrum",
     "energy_per_bond",
     "env_1site",
     "env_2sites",

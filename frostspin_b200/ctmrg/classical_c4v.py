@@ -9,6 +9,7 @@ exactly as the reference example does (:44-64, :362-384).
 
 import numpy as np
 import scipy.linalg as lg
+import torch
 
 from ..symmetric_tensor import DiagonalTensor, U1SymmetricTensor
 
@@ -107,3 +108,31 @@ def energy_per_bond(s, T, a0d, mopd):
     nr = np.einsum("abcdef,bgdc,afeg->", env2, a0d, a0d)
     sdsr = np.einsum("abcdef,bgdc,afeg->", env2, mopd, mopd)
     return -sdsr / nr
+
+
+def edge_transfer_spectrum(T, nvals=4):
+    """Leading eigenvalues (by modulus, largest first) of the edge transfer
+    operator of the C4v environment: M[(l1, l2), (r1, r2)] = sum_p T[l1, p, r1]
+    T[l2, p, r2], the chi^2 x chi^2 operator of two edge tensors contracted
+    over the physical leg.  Formed with the device block operations (one
+    grouped GEMM and one permute); its sectors are diagonalised on the device.
+    The corner representation must be self-conjugate (Z2), so that the row
+    pairs (l1, l2) and column pairs (r1, r2) of a sector are the same states in
+    the same order."""
+    Tr = T.permute((0, 2), (1,))
+    M = (Tr @ Tr.dagger()).permute((0, 2), (1, 3))
+    vals = []
+    for b in M.blocks:
+        if b.shape[0] != b.shape[1]:
+            raise ValueError("edge transfer sector is not square: corner not self-conjugate")
+        if b.shape[0]:
+            vals.append(torch.linalg.eigvals(b.contiguous()))
+    lam = torch.cat(vals).cpu().numpy()
+    return lam[np.argsort(-np.abs(lam), kind="stable")][:nvals]
+
+
+def correlation_length(T):
+    """xi = -1 / ln|lambda_2 / lambda_1| of the edge transfer operator
+    (edge_transfer_spectrum), in lattice spacings."""
+    lam = edge_transfer_spectrum(T, 2)
+    return -1.0 / np.log(abs(lam[1]) / abs(lam[0]))

@@ -17,7 +17,12 @@ from . import instrument
 # ----------------------------------------------------------------- precision
 
 _PRECISION = {"gemm": "fp64", "dispatch": "cost", "pair": True}
-PRECISIONS = ("fp64",) + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
+PRECISIONS = (
+    ("fp64",)
+    + tuple(f"ozaki{s}" for s in range(3, _native.FS_OZAKI_MAX_SLICES + 1))
+    + tuple(f"ozaki2_{n}" for n in range(_native.FS_OZAKI2_MIN_MODULI,
+                                         _native.FS_OZAKI2_MAX_MODULI + 1))
+)
 
 
 def gemm_precision():
@@ -26,9 +31,13 @@ def gemm_precision():
 
 def set_gemm_precision(mode):
     """Select the sector-GEMM arithmetic: "fp64" (plain double precision on the
-    FP64 pipes) or "ozakiS" (FP64 operands split into S int8 digit slices, exact
+    FP64 pipes), "ozakiS" (FP64 operands split into S int8 digit slices, exact
     int32 products on the tcgen05 tensor cores, FP64 recombination; relative
-    error ~2^-7S of the row/column maxima, S = 3..8)."""
+    error ~2^-7S of the row/column maxima, S = 3..8; S(S+1)/2 int8 products) or
+    "ozaki2_N" (operands rounded to scaled integers, one int8 product per
+    modulus for N = 8..14 coprime moduli, exact CRT reconstruction in FP64;
+    relative error ~2^-min(a, b) with a, b from fs_ozaki2_bits, 2^-48 at
+    N = 14 and K = 2048)."""
     if mode not in PRECISIONS:
         msg = f"unknown GEMM precision {mode!r}; choose from {PRECISIONS}"
         raise ValueError(msg)
@@ -124,6 +133,20 @@ def grouped_gemm(problems):
     if mode == "fp64":
         with instrument.region("gemm_fp64", flops=float(flops.sum())):
             _dgemm(arr, problems, tm, tn, ntile)
+    elif mode.startswith("ozaki2_"):
+        nmod = int(mode[7:])
+        fits = arr["K"].astype(np.int64) <= _native.FS_OZAKI2_MAX_K
+        if _PRECISION["dispatch"] == "all":
+            use = fits
+        else:
+            use = fits & ozaki2_pays(arr, nmod)
+        if use.any():
+            with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
+                                   int8_ops=ozaki2_int8_ops(arr[use], nmod)):
+                ozaki2_gemm(arr[use], nmod)
+        if (~use).any():
+            with instrument.region("gemm_fp64", flops=float(flops[~use].sum())):
+                _dgemm(arr[~use], None, tm, tn, ntile[~use])
     elif mode.startswith("ozaki"):
         S = int(mode[5:])
         if _PRECISION["dispatch"] == "all":
@@ -214,6 +237,27 @@ def ozaki_pays(arr, S):
     K = arr["K"].astype(np.float64)
     t_oz = (S * (S + 1) / 2 * 2 * _pad(M, 128) * _pad(N, 256) * _pad(np.maximum(K, 1), 128)
             / _INT8_OPS + S * M * N * 16 / _EPILOGUE_BPS + (M * K + K * N) * (8 + S) / _SPLIT_BPS)
+    t_64 = 2 * _pad(M, 64) * _pad(N, 64) * K / _FP64_FLOPS
+    return t_oz < t_64
+
+
+_CRT_S_PER_ENTRY = 2.0e-12   # CRT epilogue per output entry (FP64 pipe, not hidden)
+
+
+def ozaki2_int8_ops(arr, nmod):
+    M = _pad(arr["M"].astype(np.float64), 256)
+    N = _pad(arr["N"].astype(np.float64), 256)
+    K = _pad(np.maximum(arr["K"].astype(np.float64), 1), 128)
+    return float((2 * M * N * K).sum() * nmod)
+
+
+def ozaki2_pays(arr, nmod):
+    """Per problem: True when the Ozaki II path is estimated faster than FP64."""
+    M = arr["M"].astype(np.float64)
+    N = arr["N"].astype(np.float64)
+    K = arr["K"].astype(np.float64)
+    t_oz = (nmod * 2 * _pad(M, 256) * _pad(N, 256) * _pad(np.maximum(K, 1), 128) / _INT8_OPS
+            + M * N * _CRT_S_PER_ENTRY + (M * K + K * N) * (8 + nmod) / _SPLIT_BPS)
     t_64 = 2 * _pad(M, 64) * _pad(N, 64) * K / _FP64_FLOPS
     return t_oz < t_64
 
@@ -501,6 +545,104 @@ def ozaki_gemm(arr, nslices, workspace=None):
 
 
 _OZ_FLAGS = []
+
+OZ2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199)
+_OZ2_PRODUCT_BITS = {}
+
+
+def ozaki2_bits(nmod, K):
+    """(a, b) operand bits for nmod moduli and inner size K: the largest
+    (at most 50 each) with K 2^(a+b) <= P / 4, P the product of the moduli
+    (the same rule as fs_ozaki2_bits)."""
+    if nmod not in _OZ2_PRODUCT_BITS:
+        P = 1
+        for p in OZ2_MODULI[:nmod]:
+            P *= p
+        _OZ2_PRODUCT_BITS[nmod] = P.bit_length() - 1
+    K = max(int(K), 1)
+    L = _OZ2_PRODUCT_BITS[nmod] - 2 - (int(K - 1).bit_length() if K > 1 else 0)
+    return min(50, L // 2), min(50, L - L // 2)
+
+
+def ozaki2_plan(arr, nmod):
+    """Operand/problem/tile tables and the slice workspace size of the Ozaki II
+    path for a problem array (GEMM_PROBLEM_DTYPE); pointer fields are relative
+    to the workspace base.  Every problem runs on 256 x 256 CTA-pair tiles."""
+    n = arr.size
+    ops = np.zeros(2 * n, dtype=_native.OZ2_OPERAND_DTYPE)
+    probs = np.zeros(n, dtype=_native.OZ2_PROBLEM_DTYPE)
+    off = 0
+    tiles = []
+    for i in range(n):
+        M, N, K = int(arr["M"][i]), int(arr["N"][i]), int(arr["K"][i])
+        kt = max(1, (K + OZ_TILE_K - 1) // OZ_TILE_K)
+        art = 2 * ((M + 255) // 256)
+        ntn = (N + OZ_TILE_N - 1) // OZ_TILE_N
+        brt = 2 * ntn
+        a_bits, b_bits = ozaki2_bits(nmod, K)
+        a_sl, off = off, off + nmod * kt * art * OZ_TILE_BYTES
+        b_sl, off = off, off + nmod * kt * brt * OZ_TILE_BYTES
+        a_ex, off = off, off + _round_up(4 * max(M, 1), 256)
+        b_ex, off = off, off + _round_up(4 * max(N, 1), 256)
+        off = _round_up(off, 1024)
+        lda, ldb = int(arr["lda"][i]), int(arr["ldb"][i])
+        ta, tb = int(arr["transA"][i]), int(arr["transB"][i])
+        ops[2 * i] = (arr["A"][i], 1 if ta else lda, lda if ta else 1, a_sl, a_ex, M, K, art, kt,
+                      a_bits, 0)
+        ops[2 * i + 1] = (arr["B"][i], ldb if tb else 1, 1 if tb else ldb, b_sl, b_ex, N, K, brt,
+                          kt, b_bits, 0)
+        probs[i] = (a_sl, b_sl, a_ex, b_ex, arr["C"][i], arr["ldc"][i], M, N, K, art, brt, kt,
+                    arr["alpha"][i], arr["beta"][i], a_bits, b_bits)
+        for tm_ in range(art // 2):
+            for tn_ in range(ntn):
+                tiles.append((i, tm_, tn_, K))
+    table = np.zeros(len(tiles), dtype=_native.OZ_TILE_DTYPE)
+    if tiles:
+        t = np.array(tiles, dtype=np.int64)
+        t = t[np.argsort(-t[:, 3], kind="stable")]
+        table["problem"] = t[:, 0]
+        table["tm"] = t[:, 1]
+        table["tn"] = t[:, 2]
+    return ops, probs, table, off
+
+
+_OZ2_SCRATCH = {}
+
+
+def ozaki2_gemm(arr, nmod):
+    """Run the problems of `arr` (GEMM_PROBLEM_DTYPE) on the Ozaki II path
+    (fs_ozaki2_split + fs_ozaki2_gemm_pair); the slice workspace and the CRT
+    scratch come from torch's caching allocator."""
+    ops, probs, tiles, nbytes = ozaki2_plan(arr, nmod)
+    if tiles.size == 0:
+        return None
+    if nmod not in _OZ2_SCRATCH:
+        _OZ2_SCRATCH[nmod] = _native.ozaki2_scratch_bytes(nmod)
+    ws_bytes = _round_up(max(nbytes, 128 * 128), 1024)
+    scratch_bytes = _OZ2_SCRATCH[nmod]
+    buf = torch.empty(ws_bytes + scratch_bytes, dtype=torch.uint8, device=dev.device())
+    base = buf.data_ptr()
+    for f in ("slices", "exps"):
+        ops[f] += np.uint64(base)
+    for f in ("a_slices", "b_slices", "a_exps", "b_exps"):
+        probs[f] += np.uint64(base)
+    d_ops = dev.upload(ops)
+    d_probs = dev.upload(probs)
+    d_tiles = dev.upload(tiles)
+    max_rows = int(ops["rows"].max())
+    max_units = int((ops["rowtiles"].astype(np.int64) * 4 * ops["ktiles"]).max())
+    for start in range(0, ops.size, 65534):
+        cnt = min(65534, ops.size - start)
+        _native.call("fs_ozaki2_split", d_ops.data_ptr() + start * ops.itemsize, cnt, max_rows,
+                     max_units, nmod, dev.stream())
+    flag = torch.zeros(1, dtype=torch.int32, device=dev.device())
+    _native.call("fs_ozaki2_gemm_pair", d_probs.data_ptr(), probs.size, d_tiles.data_ptr(),
+                 tiles.size, nmod, base, ws_bytes, base + ws_bytes, scratch_bytes,
+                 flag.data_ptr(), dev.stream())
+    _OZ_FLAGS.append(flag)
+    if len(_OZ_FLAGS) > 64:
+        check_ozaki_flags()
+    return buf
 
 
 def check_ozaki_flags():

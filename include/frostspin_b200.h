@@ -264,6 +264,92 @@ int fs_ozaki_gemm_pair(const FsOzProblem* d_probs, int64_t n_probs,
                        int32_t chunk_ktiles, const void* d_workspace,
                        int64_t workspace_bytes, int32_t* d_flag, void* stream);
 
+/* ----------------------------- Ozaki II: CRT over int8 moduli on tcgen05 */
+/*
+ * FP64-class GEMM with one int8 tensor-core product per modulus (the
+ * integer-modular "Ozaki scheme II", Ozaki, Uchino and Imamura 2025): each row
+ * i of op(A) is scaled by 2^(a - e_i) and rounded to an integer (|A'| <= 2^a,
+ * e_i the frexp exponent of the row maximum), each column j of op(B) by
+ * 2^(b - f_j); the exact integer product X = A'B' (|X| <= K 2^(a+b) <= P/4,
+ * P the product of the nmod pairwise coprime moduli 256, 255, 253, 251, 247,
+ * 241, 239, 233, 229, 227, 223, 217, 211, 199) is rebuilt from its residues
+ * by the Chinese remainder theorem in exact FP64 arithmetic, and
+ * C = alpha X 2^(e_i + f_j - a - b) + beta C.  Relative error per entry is
+ * ~2^-min(a, b) of the product of the row/column maxima; fs_ozaki2_bits gives
+ * a and b for a modulus count and K (14 moduli, K = 2048: a = 48, b = 49).
+ * Non-finite inputs are not supported.
+ *
+ * Operands use the slice layout of the digit form: nmod residue slices of
+ * rowtiles x ktiles tiles of 128 rows x 128 bytes (128-byte swizzled, K-major),
+ * B stored transposed; every problem needs an even a_rowtiles (256-row tiles on
+ * CTA pairs) and K <= FS_OZAKI2_MAX_K (exact int32 residue products).
+ */
+#define FS_OZAKI2_MIN_MODULI 8
+#define FS_OZAKI2_MAX_MODULI 14
+#define FS_OZAKI2_MAX_K 131071
+
+typedef struct FsOz2Operand {
+    const double* src;     /* element (row, k) at src[row*s_row + k*s_k]      */
+    int64_t s_row, s_k;
+    int8_t* slices;        /* nmod*ktiles*rowtiles*16384 bytes                */
+    int32_t* exps;         /* rows entries                                    */
+    int32_t rows, K;
+    int32_t rowtiles, ktiles;
+    int32_t bits;          /* a for op(A), b for op(B)                        */
+    int32_t pad;
+} FsOz2Operand;
+
+typedef struct FsOz2Problem {
+    const int8_t* a_slices;
+    const int8_t* b_slices;
+    const int32_t* a_exps;
+    const int32_t* b_exps;
+    double* C;             /* row-major M x N, leading dimension ldc          */
+    int64_t ldc;
+    int32_t M, N, K;
+    int32_t a_rowtiles, b_rowtiles, ktiles;
+    double alpha, beta;
+    int32_t a_bits, b_bits;
+} FsOz2Problem;
+
+/* Operand bits a, b for nmod moduli and inner dimension K. */
+int fs_ozaki2_bits(int32_t nmod, int64_t K, int32_t* a_bits, int32_t* b_bits);
+
+/*
+ * The CRT constants the kernels use, for checking: the moduli, the weights
+ * W_m = (P/p_m) ((P/p_m)^-1 mod p_m) split into two doubles on the grids
+ * 2^grids[0] and 2^grids[1] (weights_hi, weights_lo; the remainder below
+ * 2^grids[1] is dropped), P split the same way (modulus_product[0..1]) and
+ * frac[m] = ((P/p_m)^-1 mod p_m) / p_m in FP32.  Host arrays of nmod entries.
+ */
+int fs_ozaki2_constants(int32_t nmod, int32_t* moduli, double* weights_hi,
+                        double* weights_lo, double* modulus_product, float* frac,
+                        int32_t* grids);
+
+/* Bytes of CRT scratch fs_ozaki2_gemm_pair needs (every CTA parks nmod
+ * residue bytes per entry of its 128 x 256 tile half). */
+int fs_ozaki2_scratch_bytes(int32_t nmod, int64_t* bytes);
+
+/* Row exponents and residue slices of every operand (grid.y = operand,
+ * <= 65535); max_units = the largest rowtiles * 4 * ktiles. */
+int fs_ozaki2_split(const FsOz2Operand* d_ops, int64_t n_ops, int32_t max_rows,
+                    int64_t max_units, int32_t nmod, void* stream);
+
+/*
+ * The Ozaki II replacement of fs_grouped_dgemm for the same call sites
+ * (symmetric_tensor.py:453-489, ctm_renormalize.py:92-94, 122-123): 256 x 256
+ * output tiles on CTA pairs (tcgen05.mma.cta_group::2 kind::i8), one TMEM
+ * accumulation per modulus, the residue reduction and the CRT in the epilogue.
+ * d_workspace holds every problem's slices (as for fs_ozaki_gemm_pair);
+ * d_scratch (fs_ozaki2_scratch_bytes, 16-byte aligned) the parked residues.
+ * A bounded wait that runs out writes FS_ERR_TIMEOUT to d_flag (if not null);
+ * a problem with K > FS_OZAKI2_MAX_K is skipped with FS_ERR_UNSUPPORTED there.
+ */
+int fs_ozaki2_gemm_pair(const FsOz2Problem* d_probs, int64_t n_probs,
+                        const FsOzTile* d_tiles, int64_t n_tiles, int32_t nmod,
+                        const void* d_workspace, int64_t workspace_bytes, void* d_scratch,
+                        int64_t scratch_bytes, int32_t* d_flag, void* stream);
+
 /*
  * Grouped Ozaki GEMM that allocates nothing.  No counterpart in the reference.
  *

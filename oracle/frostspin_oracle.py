@@ -481,3 +481,17 @@ def ising_energy_per_bond(s_blocks, s_irreps, T, a0d, mopd):
     nr = np.einsum("abcdef,bgdc,afeg->", env2, a0d, a0d)
     sdsr = np.einsum("abcdef,bgdc,afeg->", env2, mopd, mopd)
     return -sdsr / nr
+
+
+def ising_correlation_length(T):
+    """xi = -1/ln|lambda_2/lambda_1| of the C4v edge transfer operator
+    M[(l1, l2), (r1, r2)] = sum_p T[l1, p, r1] T[l2, p, r2] (dense, FP64).
+    The reference example (examples/ising_classical_ctmrg.py) computes no
+    correlation length; this restates the definition used for the Z2 Ising
+    benchmark, applied to the reference's own edge tensors."""
+    Td = toarray(T)
+    chi = Td.shape[0]
+    M = np.einsum("apc,bpd->abcd", Td, Td).reshape(chi * chi, -1)
+    lam = np.linalg.eigvals(M)
+    lam = lam[np.argsort(-np.abs(lam), kind="stable")]
+    return -1.0 / np.log(abs(lam[1]) / abs(lam[0])), lam[:4]

@@ -82,6 +82,14 @@ int main(void) {
   F(FsOzProblem, N) F(FsOzProblem, K) F(FsOzProblem, a_rowtiles) F(FsOzProblem, b_rowtiles)
   F(FsOzProblem, ktiles) F(FsOzProblem, alpha) F(FsOzProblem, beta)
   S(FsOzTile) F(FsOzTile, problem) F(FsOzTile, tm) F(FsOzTile, tn)
+  S(FsOz2Operand) F(FsOz2Operand, src) F(FsOz2Operand, s_row) F(FsOz2Operand, s_k)
+  F(FsOz2Operand, slices) F(FsOz2Operand, exps) F(FsOz2Operand, rows) F(FsOz2Operand, K)
+  F(FsOz2Operand, rowtiles) F(FsOz2Operand, ktiles) F(FsOz2Operand, bits)
+  S(FsOz2Problem) F(FsOz2Problem, a_slices) F(FsOz2Problem, b_slices)
+  F(FsOz2Problem, a_exps) F(FsOz2Problem, b_exps) F(FsOz2Problem, C) F(FsOz2Problem, ldc)
+  F(FsOz2Problem, M) F(FsOz2Problem, N) F(FsOz2Problem, K) F(FsOz2Problem, a_rowtiles)
+  F(FsOz2Problem, b_rowtiles) F(FsOz2Problem, ktiles) F(FsOz2Problem, alpha)
+  F(FsOz2Problem, beta) F(FsOz2Problem, a_bits) F(FsOz2Problem, b_bits)
   S(FsSplitReduce) F(FsSplitReduce, W) F(FsSplitReduce, C) F(FsSplitReduce, ldc)
   F(FsSplitReduce, slice) F(FsSplitReduce, nslices) F(FsSplitReduce, M)
   F(FsSplitReduce, N) F(FsSplitReduce, alpha) F(FsSplitReduce, beta)
@@ -104,6 +112,8 @@ DTYPES = {
     "FsOzOperand": _native.OZ_OPERAND_DTYPE,
     "FsOzProblem": _native.OZ_PROBLEM_DTYPE,
     "FsOzTile": _native.OZ_TILE_DTYPE,
+    "FsOz2Operand": _native.OZ2_OPERAND_DTYPE,
+    "FsOz2Problem": _native.OZ2_PROBLEM_DTYPE,
     "FsSplitReduce": _native.SPLIT_REDUCE_DTYPE,
     "FsO2Term": _native.O2_TERM_DTYPE,
     "FsO2Block": _native.O2_BLOCK_DTYPE,

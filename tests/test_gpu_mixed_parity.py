@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 SDS = np.array([[0.25, 0, 0, 0], [0, -0.25, 0.5, 0], [0, 0.5, -0.25, 0],
                 [0, 0, 0, 0.25]]).reshape(2, 2, 2, 2)
 
-MIXED = ["ozaki7"]
+MIXED = ["ozaki7", "ozaki2_13", "ozaki2_14"]
 
 
 @pytest.mark.parametrize("precision", MIXED)

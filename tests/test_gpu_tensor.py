@@ -184,3 +184,27 @@ def test_ising_chi32_100_iterations_energy():
         s, T = iterate_c4v(s, T, a, a2, 32)
     e = energy_per_bond(s, T, a0d, mopd)
     assert abs(e - float(d["energy100"])) < 1e-9
+
+
+def test_ising_chi32_correlation_length():
+    """Correlation length of the C4v Ising run (beta = 0.44, chi = 32, 100
+    iterations): xi of the device environment against xi of the reference's
+    own edge tensor after 100 iterations (the oracle's dense FP64 edge transfer
+    operator), and the device transfer spectrum of the reference's tensor
+    against the oracle's."""
+    from frostspin_b200 import DiagonalTensor
+    from frostspin_b200.ctmrg import (correlation_length, edge_transfer_spectrum,
+                                      ising_site_tensors, iterate_c4v)
+    from tests.helpers import oracle_from_dic
+
+    d = load("ising_chi32")
+    xi_ref, lam_ref = fo.ising_correlation_length(oracle_from_dic(d, "T100"))
+    lam_dev = edge_transfer_spectrum(dev_from_dic(d, "T100"), 4)
+    np.testing.assert_allclose(np.sort(np.abs(lam_dev)), np.sort(np.abs(lam_ref)), rtol=1e-12)
+    a, a2, _, _ = ising_site_tensors(float(d["beta"]))
+    s = DiagonalTensor.load_from_dic(d, prefix="s0")
+    T = dev_from_dic(d, "T0")
+    for _ in range(100):
+        s, T = iterate_c4v(s, T, a, a2, 32)
+    xi = correlation_length(T)
+    assert abs(xi - xi_ref) < 1e-6 * xi_ref, (xi, xi_ref)

@@ -149,3 +149,17 @@ def test_oracle_ctmrg_matches_reference_run():
             ref21 = d[f"it{it}_rdm2x1_{x}{y}"]
             assert np.abs(r12 - ref12).max() < tol * max(1.0, np.abs(ref12).max())
             assert np.abs(r21 - ref21).max() < tol * max(1.0, np.abs(ref21).max())
+
+
+def test_oracle_ising_correlation_length_of_reference_tensors():
+    """The oracle's C4v correlation length on the reference's own edge tensors
+    (beta = 0.44, chi = 32): it grows along the run (critical slowing near
+    beta_c = 0.4407) and the leading transfer eigenvalue is simple."""
+    from tests.helpers import load, oracle_from_dic
+
+    d = load("ising_chi32")
+    xis = [fo.ising_correlation_length(oracle_from_dic(d, f"T{it}"))[0] for it in (1, 5, 100)]
+    assert xis[0] < xis[1] < xis[2]
+    assert 50 < xis[2] < 200
+    lam = fo.ising_correlation_length(oracle_from_dic(d, "T100"))[1]
+    assert abs(lam[0]) > abs(lam[1])
