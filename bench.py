@@ -413,7 +413,7 @@ def run_ctmrg(args, world, rank, local):
     hostA = [t.data.cpu().pin_memory() for t in tensors]
     e2e_env = start_env.copy()
     linalg.set_gemm_precision(mixed if headline_mixed else "fp64")
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = args.steps
     torch.cuda.synchronize()
     es = torch.cuda.Event(enable_timing=True)
     ee = torch.cuda.Event(enable_timing=True)
@@ -429,6 +429,32 @@ def run_ctmrg(args, world, rank, local):
     t_e2e = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
     h2d = int(sum(h.numel() * 8 for h in hostA))
     d2h = int(4 * 2 * 16 * 8)  # four 2x2x2x2 reduced density matrices per site pair
+
+    # the same workload at the smaller chi the CPU arm measures, so that a
+    # same-configuration GPU/CPU ratio exists next to the chi=256 extrapolation
+    same_cfg = {}
+    for chi_c in (int(c) for c in args.compare_chis.split(",") if c):
+        from frostspin_b200.ctmrg import SequentialCTMRG
+
+        c_env = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, chi_c, cutoff=1e-10,
+                                                        degen_ratio=0.9999)
+        linalg.set_gemm_precision("fp64")
+        c_env.iterate()
+        row = {}
+        for prec in ("fp64", mixed):
+            env = c_env.copy()
+            linalg.set_gemm_precision(prec)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            env.iterate()
+            e1.record()
+            torch.cuda.synchronize()
+            row["gpu_s_per_iter_" + ("fp64" if prec == "fp64" else "mixed")] = \
+                max_over_ranks(e0.elapsed_time(e1) * 1e-3, world)
+        same_cfg[str(chi_c)] = row
+    linalg.check_ozaki_flags()
 
     hbm, bf16, peak_kind = load_peaks()
     fp64_peak = measure_dgemm_peak()
@@ -494,6 +520,7 @@ def run_ctmrg(args, world, rank, local):
                              "launches": perm["launches"], "ms": perm["ms"]},
         "e2e": {"value": world * e2e_steps / t_e2e, "unit": "iter/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "same_config_points": same_cfg,
         "gpu_launches": lmx if headline_mixed else l64,
         "clocks": clkmx if headline_mixed else clk64,
     }
@@ -503,7 +530,7 @@ def run_ctmrg(args, world, rank, local):
             info["value"] = 1.0 / t_cpu
             info["unit"] = "iter/s"
         else:
-            info = cpu_ctmrg_sample(args.symmetry, args.chi, steps=1, warmup=1)
+            info = cpu_ctmrg_sample(args.symmetry, args.chi, chis=(16, 32))
         line["cpu_baseline"] = info
     return line
 
@@ -531,36 +558,50 @@ def fixture_site_tensors(symmetry):
     return out
 
 
-def cpu_ctmrg_sample(symmetry, chi_target, *, steps, warmup, chis=(16, 32)):
+def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1):
     """Bounded CPU sample of the CTMRG workload: the numpy oracle (restating the
-    reference, BLAS on all host threads) from the reference's own site tensors,
-    `warmup` untimed then `steps` timed iterations at chis[0], one untimed and
-    one timed iteration at chis[1]; t(chi) = t(chis[1]) (chi / chis[1])^p with p
-    fitted on the two measured points, extrapolated to chi_target."""
+    reference) from the reference's own site tensors, with BLAS on every host
+    core (pinned through threadpoolctl); at each chi of `chis` one untimed
+    iteration grows the environment to that chi, then `timed` iterations are
+    timed.  The value at chi_target is a power law t = t(chis[-1]) (chi /
+    chis[-1])^p fitted on the last two measured points, labelled as an
+    extrapolation when chi_target is not among them."""
+    from threadpoolctl import threadpool_info, threadpool_limits
+
     from oracle import ctmrg_oracle as co
 
+    cores = os.cpu_count() or 1
     A, B = fixture_site_tensors(symmetry)
-    times = []
-    for chi, n_warm, n_steps in ((chis[0], warmup, steps), (chis[1], 1, 1)):
-        c = co.SequentialCTMRG(A, B, chi, cutoff=1e-10, degen_ratio=0.9999)
-        for _ in range(n_warm):
+    times = {}
+    with threadpool_limits(limits=cores):
+        threads = sorted({int(d.get("num_threads", 0)) for d in threadpool_info()})
+        for chi in chis:
+            c = co.SequentialCTMRG(A, B, chi, cutoff=1e-10, degen_ratio=0.9999)
             c.iterate()
-        t0 = time.perf_counter()
-        for _ in range(n_steps):
-            c.iterate()
-        times.append((time.perf_counter() - t0) / n_steps)
-    p = float(np.log(times[1] / times[0]) / np.log(chis[1] / chis[0]))
-    t_target = times[1] * (chi_target / chis[1]) ** max(p, 0.0)
+            t0 = time.perf_counter()
+            for _ in range(timed):
+                c.iterate()
+            times[chi] = (time.perf_counter() - t0) / timed
+    measured = chi_target in times
+    if measured:
+        t_target, p = times[chi_target], None
+    else:
+        c0, c1 = chis[-2], chis[-1]
+        p = float(np.log(times[c1] / times[c0]) / np.log(c1 / c0))
+        t_target = times[c1] * (chi_target / c1) ** max(p, 0.0)
+    pts = ", ".join(f"{v:.1f} s at chi={k}" for k, v in times.items())
     return {
-        "value": 1.0 / t_target, "unit": "iter/s", "cores": os.cpu_count() or 1,
-        "kind": "port",
+        "value": 1.0 / t_target, "unit": "iter/s", "cores": cores, "kind": "port",
+        "blas_threads": threads,
         "sample": (f"numpy oracle SequentialCTMRG ({symmetry}) from the reference's own "
-                   f"simple-update tensors (D=24 target, beta=2): {times[0]:.2f} s/iteration "
-                   f"at chi={chis[0]} (mean of {steps}), {times[1]:.2f} s at chi={chis[1]}; "
-                   f"value = power-law fit (exponent {p:.2f}) extrapolated to chi={chi_target} "
-                   f"({t_target:.0f} s/iteration), labelled as an extrapolation"),
-        "measured_s_per_iter": {str(chis[0]): times[0], str(chis[1]): times[1]},
-        "fit_exponent": p, "extrapolated": True,
+                   f"simple-update tensors (D=24 target, beta=2), BLAS on {cores} host cores; "
+                   f"one warm-up then {timed} timed iteration(s) per chi: {pts}"
+                   + ("" if measured else
+                      f"; value = power-law fit (exponent {p:.2f}) on the last two points, "
+                      f"extrapolated to chi={chi_target} ({t_target:.0f} s/iteration), "
+                      f"labelled as an extrapolation")),
+        "measured_s_per_iter": {str(k): v for k, v in times.items()},
+        "fit_exponent": p, "extrapolated": not measured,
     }
 
 
@@ -849,7 +890,8 @@ def run_gemm(args, world, rank, local):
 def run_reference_ctmrg(args, world):
     """The reference arm of the CTMRG workload: the CPU oracle port (the
     reference is Python + numba and does not travel to the GPU box)."""
-    info = cpu_ctmrg_sample(args.symmetry, args.chi, steps=args.steps, warmup=args.warmup)
+    chis = tuple(int(c) for c in args.cpu_chis.split(","))
+    info = cpu_ctmrg_sample(args.symmetry, args.chi, chis=chis)
     value = info["value"]
     return {
         "metric": METRIC,
@@ -1049,6 +1091,10 @@ def main():
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--compare-chis", default="64",
+                    help="smaller chi values also timed on the GPU (one iteration each)")
+    ap.add_argument("--cpu-chis", default="32,64",
+                    help="chi values the CPU reference arm of the ctmrg workload measures")
     ap.add_argument("--ozaki-pair", choices=["on", "off"], default="on",
                     help="large int8 sector GEMMs on CTA pairs (tcgen05 cta_group::2)")
     ap.add_argument("--precision", default="ozaki7",
@@ -1061,7 +1107,9 @@ def main():
         args.D = 24 if args.symmetry == "su2" else 12
     if args.chi is None:
         args.chi = 256 if args.symmetry == "su2" else 64
+    args.warmup_requested = args.warmup
     if args.warmup < 3:
+        # the timing rules need at least 3 untimed steps; the line reports both
         args.warmup = 3
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
@@ -1083,6 +1131,8 @@ def main():
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0:
+        if args.warmup_requested != args.warmup:
+            line["warmup_requested"] = args.warmup_requested
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

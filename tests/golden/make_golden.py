@@ -1,9 +1,9 @@
 #!/usr/bin/env python
 """Generate golden fixtures from the reference frostspin implementation.
 
-Run in a container where the reference tree is available (read-only):
+Run where the reference tree is available (read-only), naming it:
 
-    PYTHONPATH=/root/reference python -O tests/golden/make_golden.py
+    FROSTSPIN_REFERENCE=<path of the reference tree> python -O tests/golden/make_golden.py
 
 It imports frostspin 1.0.0 from that tree, builds seeded inputs, runs the
 reference's own operations and stores inputs and outputs as .npz files next to
@@ -18,7 +18,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FROSTSPIN_REFERENCE", "/root/reference")
+REF = os.environ.get("FROSTSPIN_REFERENCE")
+if not REF:
+    sys.exit("set FROSTSPIN_REFERENCE to the path of the reference (frostspin 1.0.0) tree")
 if REF not in sys.path:
     sys.path.insert(0, REF)
 
