@@ -89,6 +89,21 @@ def ozaki_pair_mode(enabled):
 
 # ------------------------------------------------------------- grouped GEMM
 
+# when a list: every grouped_gemm call appends its problem table (the shapes the
+# autotuner and the profiling scripts replay)
+_RECORDER = None
+
+
+@contextlib.contextmanager
+def record_gemm_calls():
+    """Collect the FsGemmProblem tables of every grouped_gemm call made inside."""
+    global _RECORDER
+    old, _RECORDER = _RECORDER, []
+    try:
+        yield _RECORDER
+    finally:
+        _RECORDER = old
+
 _TILE = None
 
 
@@ -127,6 +142,8 @@ def grouped_gemm(problems):
         arr["alpha"][i] = p.get("alpha", 1.0)
         arr["beta"][i] = p.get("beta", 0.0)
         ntile.append(((M + tm - 1) // tm) * ((N + tn - 1) // tn))
+    if _RECORDER is not None:
+        _RECORDER.append(arr.copy())
     mode = gemm_precision()
     ntile = np.array(ntile, dtype=np.int64)
     flops = 2.0 * (arr["M"].astype(np.float64) * arr["N"] * arr["K"])
