@@ -372,9 +372,25 @@ def run_ctmrg(args, world, rank, local):
     mixed = args.precision if args.precision != "fp64" else "ozaki7"
     su, tensors, ctm, t_su = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
-    for _ in range(args.warmup):
-        ctm.iterate()
+    for w in range(args.warmup):
+        if w == args.warmup - 1 and args.autotune == "on":
+            # the last warm-up iteration records the sector GEMM launches; the
+            # tuner measures their shape classes on both paths before timing
+            with linalg.record_gemm_calls() as records:
+                ctm.iterate()
+        else:
+            ctm.iterate()
     torch.cuda.synchronize()
+    tune_info = None
+    if args.autotune == "on" and args.precision != "fp64":
+        from frostspin_b200 import autotune
+
+        n_cls, t_tune = autotune.tune(records, mixed)
+        autotune.set_enabled(True)
+        tune_info = {"classes_measured": n_cls, "seconds": t_tune,
+                     "classes_mixed": sum(1 for (m, _), r in autotune.table().items()
+                                          if m == mixed and r["mixed"] < r["fp64"]),
+                     "classes_total": sum(1 for (m, _) in autotune.table() if m == mixed)}
     start_env = ctm.copy()
     headline_mixed = args.precision != "fp64"
     # the headline run times exactly `steps` iterations; the comparison run
@@ -502,6 +518,7 @@ def run_ctmrg(args, world, rank, local):
             "chi_values": [int(c) for c in ctm.chi_values],
             "precision": mixed if headline_mixed else "fp64",
             "ozaki_pair": args.ozaki_pair,
+            "autotune": tune_info,
             "fp64_iter_per_s": fp64_rate, "fp64_steps": n64,
             "mixed_iter_per_s": mixed_rate, "mixed_steps": nmx,
             "mixed_over_fp64": mixed_rate / fp64_rate,
@@ -1091,6 +1108,9 @@ def main():
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", choices=["on", "off"], default="on",
+                    help="measure the sector-GEMM shape classes of a warm-up iteration on "
+                         "both paths and dispatch by the measurement")
     ap.add_argument("--compare-chis", default="64",
                     help="smaller chi values also timed on the GPU (one iteration each)")
     ap.add_argument("--cpu-chis", default="32,64",

@@ -1,0 +1,143 @@
+"""Autotuner of the sector-GEMM dispatch over the sector-size histogram.
+
+One contraction gives one grouped GEMM launch of sector problems of very uneven
+sizes (irrep degeneracies).  Each problem can run on the FP64 tensor-core path
+(DMMA, 64 x 64 tiles, split-K for short launches) or on the mixed int8 path of
+the current precision mode (256 x 256 CTA-pair tiles; Ozaki I digit slices or
+Ozaki II moduli), and which one is faster depends on the shape: small M or N
+waste most of a 256-wide tile, short K leaves the int8 pipeline and the CRT
+epilogue unamortised.  The tuner measures, for every shape class present in a
+recorded set of launches (classes = the bit lengths of M, N and K), a launch of
+copies of the class's largest problem on each path with random operands, and
+keeps the seconds per FLOP; grouped_gemm then sends each problem to the path
+with the smaller predicted time.  Problems of classes that were never measured
+fall back to the analytic cost model.
+
+Typical use: record the launches of one untimed iteration
+(linalg.record_gemm_calls), then tune(records, mode) before timing.
+"""
+
+import time
+
+import numpy as np
+import torch
+
+from . import device as dev
+
+_TABLE = {}        # (mode, class) -> {"fp64": s/flop, "mixed": s/flop, "shape": (M, N, K)}
+_ENABLED = {"on": False}
+
+# a class is timed on a launch of copies of its representative problem, with N
+# cut to at most this many columns, and enough copies for two waves of tiles
+_MAX_N = 8192
+_TARGET_TILES = 2 * 148
+_MAX_BYTES = 4 << 30
+
+
+def enabled():
+    return _ENABLED["on"]
+
+
+def set_enabled(flag):
+    _ENABLED["on"] = bool(flag)
+
+
+def clear():
+    _TABLE.clear()
+
+
+def shape_class(M, N, K):
+    return (int(M).bit_length(), int(N).bit_length(), int(K).bit_length())
+
+
+def table():
+    """The measured table: {(mode, class): {"fp64": s/flop, "mixed": s/flop,
+    "shape": representative (M, N, K)}}."""
+    return dict(_TABLE)
+
+
+def _time_launch(M, N, K, ta, tb, copies, mode, reps):
+    from . import linalg
+
+    g = torch.Generator(device=dev.device())
+    g.manual_seed(M * 131 + N * 7 + K)
+    specs = []
+    for _ in range(copies):
+        dA = torch.randn(M * K, dtype=torch.float64, device=dev.device(), generator=g)
+        dB = torch.randn(K * N, dtype=torch.float64, device=dev.device(), generator=g)
+        dC = torch.empty(M * N, dtype=torch.float64, device=dev.device())
+        specs.append({"A": dA, "a_off": 0, "a_trans": ta, "B": dB, "b_off": 0, "b_trans": tb,
+                      "C": dC, "c_off": 0, "M": M, "N": N, "K": K})
+    best = float("inf")
+    for r in range(reps + 1):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        with linalg.gemm_precision_mode(mode), linalg.ozaki_dispatch_mode("all"), \
+                _bypass():
+            linalg.grouped_gemm(specs)
+        e1.record()
+        torch.cuda.synchronize()
+        if r:
+            best = min(best, e0.elapsed_time(e1) * 1e-3)
+    linalg.check_ozaki_flags()
+    return best
+
+
+class _bypass:
+    """Disables the tuned dispatch while a class is being measured."""
+
+    def __enter__(self):
+        self.old = _ENABLED["on"]
+        _ENABLED["on"] = False
+
+    def __exit__(self, *exc):
+        _ENABLED["on"] = self.old
+
+
+def tune(records, mode, *, reps=2, min_flops=1e8):
+    """Measure every shape class of the recorded launches (a list of
+    GEMM_PROBLEM_DTYPE tables) not measured yet for `mode`; returns the number
+    of classes measured and the seconds spent."""
+    reps_by_class = {}
+    for arr in records:
+        M = arr["M"].astype(np.int64)
+        N = arr["N"].astype(np.int64)
+        K = arr["K"].astype(np.int64)
+        for i in range(arr.size):
+            f = 2.0 * M[i] * N[i] * K[i]
+            if f < min_flops:
+                continue
+            key = shape_class(M[i], N[i], K[i])
+            cur = reps_by_class.get(key)
+            if cur is None or f > cur[0]:
+                reps_by_class[key] = (f, int(M[i]), int(N[i]), int(K[i]),
+                                      bool(arr["transA"][i]), bool(arr["transB"][i]))
+    t0 = time.perf_counter()
+    n = 0
+    for key, (_, M, N, K, ta, tb) in sorted(reps_by_class.items()):
+        if (mode, key) in _TABLE:
+            continue
+        Nc = min(N, _MAX_N)
+        tiles = max(1, -(-M // 256) * -(-Nc // 256))
+        per_copy = 8 * (M * K + K * Nc + M * Nc)
+        copies = int(max(1, min(-(-_TARGET_TILES // tiles), _MAX_BYTES // max(per_copy, 1))))
+        flops = 2.0 * M * Nc * K * copies
+        row = {"shape": (M, N, K), "copies": copies}
+        for path in ("fp64", mode):
+            row["fp64" if path == "fp64" else "mixed"] = (
+                _time_launch(M, Nc, K, ta, tb, copies, path, reps) / flops)
+        _TABLE[(mode, key)] = row
+        n += 1
+    return n, time.perf_counter() - t0
+
+
+def decide(arr, mode):
+    """Per problem of `arr`: True (mixed path), False (FP64) or None (class not
+    measured)."""
+    out = []
+    for i in range(arr.size):
+        row = _TABLE.get((mode, shape_class(arr["M"][i], arr["N"][i], arr["K"][i])))
+        out.append(None if row is None else bool(row["mixed"] < row["fp64"]))
+    return out

@@ -10,9 +10,8 @@ import contextlib
 import numpy as np
 import torch
 
-from . import _native
+from . import _native, autotune, instrument
 from . import device as dev
-from . import instrument
 
 # ----------------------------------------------------------------- precision
 
@@ -156,7 +155,7 @@ def grouped_gemm(problems):
         if _PRECISION["dispatch"] == "all":
             use = fits
         else:
-            use = fits & ozaki2_pays(arr, nmod)
+            use = fits & _tuned(arr, mode, ozaki2_pays(arr, nmod))
         if use.any():
             with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
                                    int8_ops=ozaki2_int8_ops(arr[use], nmod)):
@@ -169,7 +168,7 @@ def grouped_gemm(problems):
         if _PRECISION["dispatch"] == "all":
             use = np.ones(arr.size, dtype=bool)
         else:
-            use = ozaki_pays(arr, S)
+            use = _tuned(arr, mode, ozaki_pays(arr, S))
         if use.any():
             with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
                                    int8_ops=ozaki_int8_ops(arr[use], S)):
@@ -256,6 +255,16 @@ def ozaki_pays(arr, S):
             / _INT8_OPS + S * M * N * 16 / _EPILOGUE_BPS + (M * K + K * N) * (8 + S) / _SPLIT_BPS)
     t_64 = 2 * _pad(M, 64) * _pad(N, 64) * K / _FP64_FLOPS
     return t_oz < t_64
+
+
+def _tuned(arr, mode, model):
+    """The autotuner's per-problem choice where it measured the shape class,
+    the cost model's elsewhere."""
+    if not autotune.enabled():
+        return model
+    dec = autotune.decide(arr, mode)
+    return np.array([m if d is None else d for d, m in zip(dec, model, strict=True)],
+                    dtype=bool)
 
 
 _CRT_S_PER_ENTRY = 2.0e-12   # CRT epilogue per output entry (FP64 pipe, not hidden)

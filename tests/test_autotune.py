@@ -1,0 +1,38 @@
+"""The autotuner's dispatch rule (frostspin_b200/autotune.py) on a hand-made
+table: measured classes follow the measurement, unmeasured ones the cost
+model.  Measuring needs a GPU; the rule does not."""
+
+import numpy as np
+
+from frostspin_b200 import _native, autotune, linalg
+
+
+def _arr(shapes):
+    arr = np.zeros(len(shapes), dtype=_native.GEMM_PROBLEM_DTYPE)
+    for i, (m, n, k) in enumerate(shapes):
+        arr["M"][i], arr["N"][i], arr["K"][i] = m, n, k
+    return arr
+
+
+def test_decide_uses_measured_classes_only():
+    autotune.clear()
+    arr = _arr([(3000, 3000, 3000), (100, 5000, 40), (7, 7, 7)])
+    mode = "ozaki2_13"
+    autotune._TABLE[(mode, autotune.shape_class(3000, 3000, 3000))] = {
+        "fp64": 3e-14, "mixed": 1e-14, "shape": (3000, 3000, 3000)}
+    autotune._TABLE[(mode, autotune.shape_class(100, 5000, 40))] = {
+        "fp64": 1e-13, "mixed": 4e-13, "shape": (100, 5000, 40)}
+    assert autotune.decide(arr, mode) == [True, False, None]
+    model = np.array([False, True, True])
+    autotune.set_enabled(True)
+    try:
+        assert list(linalg._tuned(arr, mode, model)) == [True, False, True]
+    finally:
+        autotune.set_enabled(False)
+        autotune.clear()
+    assert list(linalg._tuned(arr, mode, model)) == [False, True, True]
+
+
+def test_shape_classes_are_bit_lengths():
+    assert autotune.shape_class(1, 2, 3) == (1, 2, 2)
+    assert autotune.shape_class(255, 256, 257) == (8, 9, 9)
