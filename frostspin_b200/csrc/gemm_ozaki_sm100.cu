@@ -672,18 +672,25 @@ __device__ __forceinline__ double int_to_double(int32_t v) {
 
 constexpr double kRoundMagic = 6755399441055744.0;   // 1.5 * 2^52: x + M rounds x to an integer
 
-// symmetric residue of the int32 accumulator acc modulo the odd modulus p,
-// as the low byte of acc - p * rint(acc / p) (the quotient is exact: |acc/p| <
-// 2^24 and acc/p is at least 1/(2p) away from any half integer)
+// symmetric residue r of the int32 accumulator acc modulo the odd modulus p,
+// parked as the byte r + 128: the low byte of acc - p * rint(acc / p) + 128
+// (the quotient is exact: |acc/p| < 2^24 and acc/p is at least 1/(2p) away
+// from any half integer)
 __device__ __forceinline__ uint32_t residue_byte(int32_t acc, int32_t p, double inv_p) {
     const int32_t q = __double2loint(fma(int_to_double(acc), inv_p, kRoundMagic));
-    return static_cast<uint32_t>(acc - q * p) & 0xFFu;
+    return static_cast<uint32_t>(acc - q * p + 128) & 0xFFu;
+}
+
+// the exact double value of a byte u (0..255) without the conversion unit
+__device__ __forceinline__ double byte_to_double(uint32_t u) {
+    return __hiloint2double(0x43380000, static_cast<int>(u)) - kRoundMagic;
 }
 
 // CRT constants of one modulus count (host computed, passed by value): the
 // moduli, 1/p_m rounded, y_m / p_m (y_m = (P/p_m)^-1 mod p_m) as FP32, the CRT
 // weights W_m = (P/p_m) y_m split as w1_m + w2_m + (dropped) on the grids 2^e1
-// and 2^e2, and P split the same way.
+// and 2^e2, P split the same way, the offsets that undo the +128 of the parked
+// residue bytes, and 1/P.
 struct CrtConsts {
     int32_t n, e1, e2, pad;
     int32_t p[FS_OZAKI2_MAX_MODULI];
@@ -692,6 +699,8 @@ struct CrtConsts {
     double w1[FS_OZAKI2_MAX_MODULI];
     double w2[FS_OZAKI2_MAX_MODULI];
     double p1, p2;
+    double c1, c2;      // -128 sum_m w1_m and -128 sum_m w2_m (the byte offsets)
+    double inv_P;       // 1 / P rounded
 };
 
 // ------------------------------------------------ Ozaki II (CRT over moduli)
@@ -707,7 +716,7 @@ struct CrtConsts {
 // residue product is one int8 GEMM of the symmetric residues of A' and B'
 // (entries in [-128, 127], exact int32 accumulation for K < 2^17).  The CRT
 // then gives X = sum_m r_m W_m - k P with W_m = (P/p_m) ((P/p_m)^-1 mod p_m),
-// k = rint(sum_m r_m y_m / p_m), evaluated exactly in FP64 by splitting every
+// k = rint(sum_m r_m W_m / P), evaluated exactly in FP64 by splitting every
 // W_m (and P) into two doubles on fixed binary grids 2^E1 and 2^E2 so that
 // every product and partial sum is representable; the dropped remainder is
 // below 2^(E2 + 12), far under the rounding of A and B.  C = alpha X 2^(e_i +
@@ -746,32 +755,24 @@ __device__ __forceinline__ void crt_store_row(const Prob& p, const CrtConsts& cc
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             if (j < ncol) {
-                // k = rint(sum_m r_m y_m / p_m) in FP32: |sum| < 2^12 and the
-                // rounding errors stay below 1/100, while the fractional part
-                // X / P is within 1/4 of an integer
-                float kf = 0.0f;
+                // the residues arrive as bytes u_m = r_m + 128; the constant
+                // terms c1, c2 remove the offsets.  d1 = sum_m r_m w1_m and
+                // d2 = sum_m r_m w2_m are exact on their grids; d1 / P is
+                // within 2^-40 of S / P = k + X / P with |X / P| <= 1/4, which
+                // gives k, and then X = (d1 - k p1) + (d2 - k p2)
+                double d1 = cc.c1;
+                double d2 = cc.c2;
 #pragma unroll
                 for (int m = 0; m < kCrtMaxModuli; ++m) {
                     if (m < n) {
-                        const int32_t r =
-                            static_cast<int32_t>(static_cast<int8_t>(w[m][j / 4] >> (8 * (j % 4))));
-                        kf = fmaf(__int_as_float(0x4B400000 + r) - 12582912.0f, cc.f[m], kf);
+                        const double u = byte_to_double((w[m][j / 4] >> (8 * (j % 4))) & 0xFFu);
+                        d1 = fma(u, cc.w1[m], d1);
+                        d2 = fma(u, cc.w2[m], d2);
                     }
                 }
-                const int32_t k = __float_as_int(kf + 12582912.0f) - 0x4B400000;
-                const double kd = int_to_double(k);
-                double d1 = -kd * cc.p1;
-                double d2 = -kd * cc.p2;
-#pragma unroll
-                for (int m = 0; m < kCrtMaxModuli; ++m) {
-                    if (m < n) {
-                        const int32_t r =
-                            static_cast<int32_t>(static_cast<int8_t>(w[m][j / 4] >> (8 * (j % 4))));
-                        const double rd = int_to_double(r);
-                        d1 = fma(rd, cc.w1[m], d1);
-                        d2 = fma(rd, cc.w2[m], d2);
-                    }
-                }
+                const double kd = fma(d1, cc.inv_P, kRoundMagic) - kRoundMagic;
+                d1 = fma(-kd, cc.p1, d1);
+                d2 = fma(-kd, cc.p2, d2);
                 const double x = d1 + d2;
                 const double val = p.alpha * scale2(x, sa + __ldg(be + j));
                 double* dst = crow + col0 + cb + j;
@@ -987,9 +988,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         tmem_ld16(taddr + cb, v);
                         uint32_t w[4] = {0, 0, 0, 0};
                         if (g == 0) {
-                            // p = 256: the low byte is the symmetric residue
+                            // p = 256: the low byte of acc + 128 is the
+                            // symmetric residue plus 128
 #pragma unroll
-                            for (int j = 0; j < 16; ++j) w[j / 4] |= (v[j] & 0xFFu) << (8 * (j % 4));
+                            for (int j = 0; j < 16; ++j)
+                                w[j / 4] |= ((v[j] + 128u) & 0xFFu) << (8 * (j % 4));
                         } else {
 #pragma unroll
                             for (int j = 0; j < 16; ++j)
@@ -1326,6 +1329,16 @@ bool make_crt_consts(int n, fsb::oz::CrtConsts* c) {
     const u128 p1 = (P >> e1) << e1;
     c->p1 = std::ldexp(static_cast<double>(static_cast<uint64_t>(P >> e1)), e1);
     c->p2 = std::ldexp(static_cast<double>(static_cast<uint64_t>((P - p1) >> e2)), e2);
+    // the offsets are exact: 128 sum_m w1_m stays on the 2^e1 grid below
+    // 2^(53 + e1) (likewise for w2), and are added first
+    double s1 = 0.0, s2 = 0.0;
+    for (int m = 0; m < n; ++m) {
+        s1 += c->w1[m];
+        s2 += c->w2[m];
+    }
+    c->c1 = -128.0 * s1;
+    c->c2 = -128.0 * s2;
+    c->inv_P = 1.0 / std::ldexp(static_cast<double>(static_cast<uint64_t>(P >> e1)), e1);
     return true;
 }
 
