@@ -855,7 +855,7 @@ def run_ours(args, world, rank, local):
 
 
 def run_gemm(args, world, rank, local):
-    """One square FP64 GEMM (n = --gemm-n) through the grouped sector-GEMM path
+    """One FP64 GEMM (n^3 with n = --gemm-n, or --gemm-shape M,N,K) through the grouped sector-GEMM path
     at --precision (fp64: DMMA; ozakiS: tcgen05 int8, every problem on the int8
     path), timed with CUDA events beside cuBLAS DGEMM on the same operands."""
     import torch
@@ -863,12 +863,13 @@ def run_gemm(args, world, rank, local):
     from frostspin_b200 import linalg
 
     n = args.gemm_n
+    M, N, K = (int(x) for x in args.gemm_shape.split(",")) if args.gemm_shape else (n, n, n)
     g = torch.Generator(device="cuda").manual_seed(SEED)
-    A = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
-    B = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
-    C = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(K, N, dtype=torch.float64, device="cuda", generator=g)
+    C = torch.empty(M, N, dtype=torch.float64, device="cuda")
     spec = [{"A": A.reshape(-1), "a_off": 0, "a_trans": False, "B": B.reshape(-1), "b_off": 0,
-             "b_trans": False, "C": C.reshape(-1), "c_off": 0, "M": n, "N": n, "K": n}]
+             "b_trans": False, "C": C.reshape(-1), "c_off": 0, "M": M, "N": N, "K": K}]
 
     def step():
         with linalg.gemm_precision_mode(args.precision), linalg.ozaki_dispatch_mode("all"):
@@ -889,16 +890,16 @@ def run_gemm(args, world, rank, local):
 
     t = max_over_ranks(timed(step), world)
     linalg.check_ozaki_flags()
-    err = float((C - A @ B).abs().max() / (A.abs().max() * B.abs().max() * n))
+    err = float((C - A @ B).abs().max() / (A.abs().max() * B.abs().max() * K))
     t_cublas = timed(lambda: torch.matmul(A, B, out=C))
-    flops = 2.0 * n**3
+    flops = 2.0 * M * N * K
     return {
         "metric": "square GEMM, effective FP64 TFLOP/s", "value": world * flops / t / 1e12,
         "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else f"f64 via int8 {args.precision}",
         "data": "synthetic (seeded N(0,1))", "impl": "ours",
-        "config": {"workload": "gemm", "n": n, "precision": args.precision,
+        "config": {"workload": "gemm", "shape": [M, N, K], "precision": args.precision,
                    "cublas_dgemm_tflops": flops / t_cublas / 1e12,
                    "max_err_rel_to_maxA_maxB_n": err},
     }
@@ -1101,6 +1102,7 @@ def main():
     ap.add_argument("--workload", choices=["ctmrg", "u1_microbench", "gemm", "ising"],
                     default="ctmrg")
     ap.add_argument("--gemm-n", type=int, default=4096, help="matrix size of the gemm workload")
+    ap.add_argument("--gemm-shape", default=None, help="M,N,K of the gemm workload (else n,n,n)")
     ap.add_argument("--symmetry", choices=["u1", "su2"], default="su2")
     ap.add_argument("--D", type=int, default=None,
                     help="simple-update bond dimension target (default 12 for U(1), 24 for SU(2))")
