@@ -735,9 +735,12 @@ __device__ __forceinline__ void crt_store_row(const Prob& p, const CrtConsts& cc
                                               const uint8_t* scratch, int64_t row, int col0,
                                               int ea) {
     const int n = cc.n;
-    double* crow = p.C + row * p.ldc;
+    double* crow = p.C + row * p.ldc + col0;
     const int sa = ea - p.a_bits - p.b_bits;
-    for (int cb = 0; cb < kTileN && col0 + cb < p.N; cb += 16) {
+    const int ncols = min(kTileN, p.N - col0);
+    for (int cb = 0; cb < ncols; cb += 16) {
+        // every load of the chunk first (parked residues, column exponents,
+        // and C when beta != 0), so that their latencies overlap
         uint32_t w[kCrtMaxModuli][4];
 #pragma unroll
         for (int m = 0; m < kCrtMaxModuli; ++m) {
@@ -750,35 +753,46 @@ __device__ __forceinline__ void crt_store_row(const Prob& p, const CrtConsts& cc
                 w[m][3] = q.w;
             }
         }
-        const int ncol = min(16, p.N - col0 - cb);
+        const int ncol = min(16, ncols - cb);
         const int32_t* be = p.b_exps + col0 + cb;
+        int eb[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) eb[j] = (j < ncol) ? __ldg(be + j) : 0;
+        double old[16];
+        if (p.beta != 0.0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) old[j] = (j < ncol) ? crow[cb + j] : 0.0;
+        }
+        double val[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-            if (j < ncol) {
-                // the residues arrive as bytes u_m = r_m + 128; the constant
-                // terms c1, c2 remove the offsets.  d1 = sum_m r_m w1_m and
-                // d2 = sum_m r_m w2_m are exact on their grids; d1 / P is
-                // within 2^-40 of S / P = k + X / P with |X / P| <= 1/4, which
-                // gives k, and then X = (d1 - k p1) + (d2 - k p2)
-                double d1 = cc.c1;
-                double d2 = cc.c2;
+            // the residues arrive as bytes u_m = r_m + 128; the constant terms
+            // c1, c2 remove the offsets.  d1 = sum_m r_m w1_m and d2 = sum_m
+            // r_m w2_m are exact on their grids; d1 / P is within 2^-29 of
+            // S / P = k + X / P with |X / P| <= 1/4, which gives k, and then
+            // X = (d1 - k p1) + (d2 - k p2)
+            double d1 = cc.c1;
+            double d2 = cc.c2;
 #pragma unroll
-                for (int m = 0; m < kCrtMaxModuli; ++m) {
-                    if (m < n) {
-                        const double u = byte_to_double((w[m][j / 4] >> (8 * (j % 4))) & 0xFFu);
-                        d1 = fma(u, cc.w1[m], d1);
-                        d2 = fma(u, cc.w2[m], d2);
-                    }
+            for (int m = 0; m < kCrtMaxModuli; ++m) {
+                if (m < n) {
+                    const double u = byte_to_double((w[m][j / 4] >> (8 * (j % 4))) & 0xFFu);
+                    d1 = fma(u, cc.w1[m], d1);
+                    d2 = fma(u, cc.w2[m], d2);
                 }
-                const double kd = fma(d1, cc.inv_P, kRoundMagic) - kRoundMagic;
-                d1 = fma(-kd, cc.p1, d1);
-                d2 = fma(-kd, cc.p2, d2);
-                const double x = d1 + d2;
-                const double val = p.alpha * scale2(x, sa + __ldg(be + j));
-                double* dst = crow + col0 + cb + j;
-                *dst = (p.beta == 0.0) ? val : fma(p.beta, *dst, val);
             }
+            const double kd = fma(d1, cc.inv_P, kRoundMagic) - kRoundMagic;
+            d1 = fma(-kd, cc.p1, d1);
+            d2 = fma(-kd, cc.p2, d2);
+            val[j] = p.alpha * scale2(d1 + d2, sa + eb[j]);
         }
+        if (p.beta != 0.0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) val[j] = fma(p.beta, old[j], val[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (j < ncol) crow[cb + j] = val[j];
     }
 }
 

@@ -839,6 +839,57 @@ def case_o2():
     save("o2", data)
 
 
+def case_checkpoints():
+    """Checkpoint interchange: files written by the reference's own
+    save_to_file (SequentialCTMRG, abstract_ctmrg.py:194-216 with
+    ctm_environment.py:262-276; SimpleUpdate, abstract_simple_update.py:149-187)
+    copied as fixtures, plus what the reference computes after reloading them
+    with its own load_from_file and continuing."""
+    import shutil
+    import tempfile
+
+    from frostspin.ctmrg import SequentialCTMRG
+    from frostspin.simple_update import SimpleUpdate
+
+    tmp = tempfile.mkdtemp()
+    expect = {}
+    d = np.load(os.path.join(HERE, "ctmrg_u1_random.npz"))
+    tensors = [U1SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A", "B")]
+    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 20, cutoff=1e-10,
+                                                  degen_ratio=0.9999)
+    for _ in range(2):
+        ctm.iterate()
+    f = os.path.join(tmp, "ctm.npz")
+    ctm.save_to_file(f)
+    shutil.copy(f, os.path.join(HERE, "ckpt_ctmrg_u1.npz"))
+    ctm2 = SequentialCTMRG.load_from_file(f)
+    ctm2.iterate()
+    expect["ctm_chi"] = np.array(ctm2.chi_values)
+    for (x, y) in ctm2.site_coords:
+        expect[f"ctm_rdm1x2_{x}{y}"] = ctm2.compute_rdm1x2(x, y).toarray()
+        expect[f"ctm_rdm2x1_{x}{y}"] = ctm2.compute_rdm2x1(x, y).toarray()
+    expect["ctm_logZ"] = np.array(ctm2.compute_PEPS_norm_log())
+
+    reps = (np.array([1, -1], dtype=np.int8),) * 2
+    h = U1SymmetricTensor.from_array(SDS_22.reshape(2, 2, 2, 2), reps, reps)
+    su = SimpleUpdate.square_lattice_first_neighbor(h, 6, 0.01, rcutoff=1e-10,
+                                                    degen_ratio=0.9999)
+    su.evolve(0.2)
+    f = os.path.join(tmp, "su.npz")
+    su.save_to_file(f)
+    shutil.copy(f, os.path.join(HERE, "ckpt_su_u1.npz"))
+    su2 = SimpleUpdate.load_from_file(f)
+    su2.evolve(0.2)
+    expect["su_beta"] = np.array(su2.beta)
+    expect["su_logZ"] = np.array(su2.logZ)
+    for i, w in enumerate(su2.get_weights()):
+        expect[f"su_w{i}"] = w
+    for i, r in enumerate(su2.get_bond_representations()):
+        expect[f"su_rep{i}"] = r
+    save("ckpt_expect", expect)
+    shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
