@@ -1165,6 +1165,8 @@ def main():
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fused-permute", choices=["on", "off"], default="on",
+                    help="thin SU(2) simple blocks in the one-pass fused permute kernel")
     ap.add_argument("--autotune", choices=["on", "off"], default="on",
                     help="measure the sector-GEMM shape classes of a warm-up iteration on "
                          "both paths and dispatch by the measurement")
@@ -1199,6 +1201,9 @@ def main():
     from frostspin_b200 import linalg
 
     linalg.set_ozaki_pair(args.ozaki_pair == "on")
+    from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor
+
+    lie_group_symmetric_tensor.set_fused_permute(args.fused_permute == "on")
     if args.workload == "ctmrg":
         line = run_ctmrg(args, world, rank, local)
     elif args.workload == "gemm":

@@ -38,6 +38,39 @@ PERM_TASK_DTYPE = np.dtype(
     [("eb", "<i4"), ("start", "<u4"), ("count", "<u4"), ("pad", "<u4")]
 )
 
+FS_SU2_MAXD = 8
+
+SU2_GROUP_DTYPE = np.dtype(
+    [
+        ("u_off", "<i8"),
+        ("ncols", "<i8"),
+        ("dims", "<u4", (FS_SU2_MAXD,)),
+        ("divm", "<u4", (FS_SU2_MAXD,)),
+        ("divs", "<u4", (FS_SU2_MAXD,)),
+        ("ndim", "<i4"),
+        ("M", "<i4"),
+        ("K", "<i4"),
+        ("in_first", "<i4"),
+        ("in_count", "<i4"),
+        ("out_first", "<i4"),
+        ("out_count", "<i4"),
+        ("pad", "<i4"),
+    ]
+)
+
+SU2_PIECE_DTYPE = np.dtype(
+    [
+        ("base", "<i8"),
+        ("sr_stride", "<i8"),
+        ("sc_stride", "<i8"),
+        ("ext", "<i8", (FS_SU2_MAXD,)),
+        ("sr", "<i4"),
+        ("sc", "<i4"),
+        ("row0", "<i4"),
+        ("pad", "<i4"),
+    ]
+)
+
 GEMM_PROBLEM_DTYPE = np.dtype(
     [
         ("A", "<u8"),
@@ -218,6 +251,9 @@ SIGNATURES = {
         ctypes.c_int,
         [_P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
     ),
+    "fs_su2_fused_limits": (ctypes.c_int, [_P, _P, _P]),
+    "fs_su2_permute_fused": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _I64,
+                                            _P, _I64, _P, _P]),
     "fs_dgemm_tile_shape": (ctypes.c_int, [_P, _P]),
     "fs_grouped_dgemm": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
     "fs_thin_dgemm_shape": (ctypes.c_int, [_P, _P, _P]),
@@ -288,7 +324,7 @@ CALL_COUNTS = {}
 
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
-    "fs_abelian_permute": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
+    "fs_abelian_permute": 1, "fs_su2_permute_fused": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
     "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2,
     "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1, "fs_ozaki2_split": 2, "fs_ozaki2_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
@@ -352,3 +388,11 @@ def ozaki2_scratch_bytes(nmod):
     n = ctypes.c_int64()
     call("fs_ozaki2_scratch_bytes", nmod, ctypes.byref(n))
     return n.value
+
+
+def su2_fused_limits():
+    """(max rows M = K, max pieces per side, threads per CTA) of the fused
+    SU(2) permute kernel."""
+    a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    call("fs_su2_fused_limits", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value

@@ -35,11 +35,26 @@ import numpy as np
 from .. import _native, instrument, linalg
 from .. import device as dev
 from .._native import FS_PERM_MAXR
+from . import su2_fused_plan
 from .abelian_plan import _make_tasks, _pack_ebs
 from .symmetric_tensor import SymmetricTensor
 
 _MAP_CACHE = OrderedDict()
 _MAP_CACHE_SIZE = 256
+_FUSED = {"on": True, "limits": None}
+
+
+def set_fused_permute(enabled):
+    """Whether permutes run the simple blocks with small recoupling matrices
+    through the one-pass fused kernel (default) or through gather -> grouped
+    GEMM -> scatter like the others; the results agree to rounding."""
+    _FUSED["on"] = bool(enabled)
+
+
+def _fused_limits():
+    if _FUSED["limits"] is None:
+        _FUSED["limits"] = _native.su2_fused_limits()
+    return _FUSED["limits"]
 
 
 # ------------------------------------------------------------------ helpers
@@ -139,23 +154,35 @@ class LieMap:
     __slots__ = (
         "gather", "scatter", "x_size", "out_size", "zero_out", "M", "N", "K",
         "u_off", "x_off", "u_host", "device", "out_offsets", "out_shapes",
-        "out_irreps", "in_len",
+        "out_irreps", "in_len", "fused", "fused_coeffs",
     )
 
     def run(self, src, out=None):
         if self.device is None:
+            fz = self.fused
             self.device = (
                 dev.upload(self.gather[0]), dev.upload(self.gather[1]),
                 dev.upload(self.scatter[0]), dev.upload(self.scatter[1]),
                 dev.upload_f64(self.u_host),
+                None if fz is None else tuple(dev.upload(a) for a in fz),
             )
-        g_ebs, g_tasks, s_ebs, s_tasks, d_u = self.device
+        g_ebs, g_tasks, s_ebs, s_tasks, d_u, d_fz = self.device
         if out is None:
             out = dev.zeros_f64(self.out_size) if self.zero_out else dev.empty_f64(self.out_size)
-        if self.x_size == 0:
-            return out
         if src.numel() < self.in_len:
             raise ValueError("source buffer is smaller than the plan expects")
+        if d_fz is not None:
+            d_groups, d_pieces, d_tasks = d_fz
+            with instrument.region("permute_fused", bytes=16.0 * self.fused_coeffs):
+                _native.call(
+                    "fs_su2_permute_fused", dev.ptr(src), int(src.numel()), dev.ptr(out),
+                    int(out.numel()), d_groups.data_ptr(), int(self.fused[0].size),
+                    d_pieces.data_ptr(), int(self.fused[1].size), d_u.data_ptr(),
+                    int(self.u_host.size), d_tasks.data_ptr(), int(self.fused[2].size), None,
+                    dev.stream(),
+                )
+        if self.x_size == 0:
+            return out
         x = dev.empty_f64(self.x_size)
         y = dev.empty_f64(int((self.M * self.N).sum()))
         with instrument.region("permute", bytes=16.0 * self.x_size):
@@ -534,7 +561,7 @@ class LieGroupSymmetricTensor(NonAbelianSymmetricTensor):
 
     def _permute_map(self, axes, new_nrr):
         key = ("permute", type(self).__name__, self._irreps_key(), self._layout_key(),
-               self._signature.tobytes(), self._nrr, axes, new_nrr)
+               self._signature.tobytes(), self._nrr, axes, new_nrr, _FUSED["on"])
         m = _MAP_CACHE.get(key)
         if m is not None:
             _MAP_CACHE.move_to_end(key)
@@ -574,39 +601,58 @@ class LieGroupSymmetricTensor(NonAbelianSymmetricTensor):
         out_sizes = out_shapes[:, 0] * out_shapes[:, 1]
         out_offsets = _exclusive_cumsum(out_sizes)
         out_size = int(out_sizes.sum())
-        x_off = _exclusive_cumsum(st["K"] * E)
-        x_size = int((st["K"] * E).sum())
+        n_sb = E.size
+        e_out = e[:, ax]
+        if _FUSED["on"] and n_sb:
+            max_rows, max_pieces, _ = _fused_limits()
+            fz = su2_fused_plan.fusable(
+                st["M"], st["K"], E, e_out, np.bincount(st["in_sb"], minlength=n_sb),
+                np.bincount(st["out_sb"], minlength=n_sb), max_rows, max_pieces)
+        else:
+            fz = np.zeros(n_sb, dtype=bool)
+        rest = ~fz
+        # X and Y hold the simple blocks that go through the grouped GEMM only
+        x_off = _exclusive_cumsum(st["K"] * E * rest)
+        x_size = int((st["K"] * E * rest).sum())
 
         sb = st["in_sb"]
         b = st["in_b"]
         src_off, rs, cs, present = self._block_source_arrays(src_block[b])
-        gather = _copy_tables(
-            *_block_gather(
-                e[sb], nrr, ax, st["in_sr"], st["in_sc"], row_start[st["ir"][sb], b],
-                col_start[st["ic"][sb], b], src_off, rs, cs, present, x_off[sb],
-                st["in_koff"], E[sb],
-            ),
-            int(self._data.numel()), x_size,
+        raw_g = _block_gather(
+            e[sb], nrr, ax, st["in_sr"], st["in_sc"], row_start[st["ir"][sb], b],
+            col_start[st["ic"][sb], b], src_off, rs, cs, present, x_off[sb],
+            st["in_koff"], E[sb],
         )
+        sel = rest[sb]
+        gather = _copy_tables(*(a[sel] for a in raw_g), int(self._data.numel()), x_size)
         sb = st["out_sb"]
         b = st["out_b"]
-        scatter = _copy_tables(
-            *_block_scatter(
-                e[sb][:, ax], new_nrr, st["out_sr"], st["out_sc"],
-                orow_start[st["ir_out"][sb], b], ocol_start[st["ic_out"][sb], b],
-                out_offsets[b], out_shapes[b, 1], x_off[sb], st["out_moff"], E[sb],
-            ),
-            x_size, out_size,  # M == K: Y has the layout of X
+        raw_s = _block_scatter(
+            e_out[sb], new_nrr, st["out_sr"], st["out_sc"],
+            orow_start[st["ir_out"][sb], b], ocol_start[st["ic_out"][sb], b],
+            out_offsets[b], out_shapes[b, 1], x_off[sb], st["out_moff"], E[sb],
         )
+        sel = rest[sb]
+        # M == K: Y has the layout of X
+        scatter = _copy_tables(*(a[sel] for a in raw_s), x_size, out_size)
+        fused, fused_coeffs = None, 0
+        if fz.any():
+            fused = su2_fused_plan.build(
+                np.flatnonzero(fz), e_out, E, st["M"], st["K"], st["u_off"], raw_g,
+                st["in_sb"], st["in_koff"], raw_s, st["out_sb"], st["out_moff"], ax)
+            su2_fused_plan.check(fused[0], fused[1], int(self._data.numel()), out_size,
+                                 int(st["u_host"].size))
+            fused_coeffs = int((st["M"] * E)[fz].sum())
         if int(gather[0]["volume"].astype(np.int64).sum()) != x_size or int(
             scatter[0]["volume"].astype(np.int64).sum()
-        ) != out_size:
+        ) + fused_coeffs != out_size:
             raise AssertionError("permute tables do not cover their buffers")
         m = LieMap()
         m.gather, m.scatter = gather, scatter
         m.x_size, m.out_size, m.zero_out = x_size, out_size, False
-        m.M, m.N, m.K = st["M"], E, st["K"]
-        m.u_off, m.x_off, m.u_host = st["u_off"], x_off, st["u_host"]
+        m.M, m.N, m.K = st["M"][rest], E[rest], st["K"][rest]
+        m.u_off, m.x_off, m.u_host = st["u_off"][rest], x_off[rest], st["u_host"]
+        m.fused, m.fused_coeffs = fused, fused_coeffs
         m.device = None
         m.out_offsets, m.out_shapes, m.out_irreps = out_offsets, out_shapes, st["bi_out"]
         m.in_len = int(self._data.numel())
@@ -767,6 +813,7 @@ class LieGroupSymmetricTensor(NonAbelianSymmetricTensor):
         ident = np.arange(ndim, dtype=np.int64)
         irr_dims = st["dims"]
         m = LieMap()
+        m.fused, m.fused_coeffs = None, 0
         if to_dense:
             # the targets are the stored blocks: sector b reads stored block b
             src_off, rs, cs, present = tensor._block_source_arrays(b)

@@ -106,6 +106,56 @@ int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_out,
                        const FsPermTask* d_tasks, int64_t n_tasks,
                        int32_t* d_flag, void* stream);
 
+/* -------------------------------------------------- fused SU(2) permute */
+/*
+ * Replaces LieGroupSymmetricTensor._lie_permute_data -> fill_blocks_out ->
+ * permute_simple_block (frostspin/symmetric_tensor/lie_group_symmetric_tensor.py
+ * :96-265, :735-835) for the simple blocks whose recoupling matrix is at most
+ * 32 x 32: gather, recoupling product and scatter in one pass.
+ *
+ * A group is one simple block: K input rows (input sectors x structural
+ * multiplicities), M output rows, ncols columns = the external multi-index in
+ * output leg order (dims, outer to inner, with Granlund-Montgomery divm / divs
+ * per leg as in FsPermEB), and U (M x K, row-major) at u_off in the U buffer.
+ * A piece is one sector's share of a group: rows row0 .. row0 + sr*sc - 1 of
+ * the group (structural index sr outer), at element base + r*sr_stride +
+ * c*sc_stride + sum_l e_l*ext[l] of its buffer for column multi-index e.  An
+ * input piece with base < 0 is an absent source block (zeros).  Pieces
+ * in_first .. in_first + in_count - 1 are the group's inputs, out_first .. its
+ * outputs.  Tasks are FsPermTask with eb = group index, start = first column,
+ * count = number of columns.  Limits: fs_su2_fused_limits.  Accesses outside
+ * a buffer are skipped and raise FS_ERR_BOUNDS in *d_flag (if not null).
+ */
+#define FS_SU2_MAXD 8
+
+typedef struct FsSu2Group {
+    int64_t u_off;
+    int64_t ncols;
+    uint32_t dims[FS_SU2_MAXD];
+    uint32_t divm[FS_SU2_MAXD];
+    uint32_t divs[FS_SU2_MAXD];
+    int32_t ndim, M, K;
+    int32_t in_first, in_count, out_first, out_count;
+    int32_t pad;
+} FsSu2Group;
+
+typedef struct FsSu2Piece {
+    int64_t base;
+    int64_t sr_stride, sc_stride;
+    int64_t ext[FS_SU2_MAXD];
+    int32_t sr, sc;
+    int32_t row0;
+    int32_t pad;
+} FsSu2Piece;
+
+int fs_su2_fused_limits(int32_t* max_rows, int32_t* max_pieces, int32_t* threads);
+
+int fs_su2_permute_fused(const double* d_src, int64_t src_len, double* d_out, int64_t out_len,
+                         const FsSu2Group* d_groups, int64_t n_groups,
+                         const FsSu2Piece* d_pieces, int64_t n_pieces, const double* d_u,
+                         int64_t u_len, const FsPermTask* d_tasks, int64_t n_tasks,
+                         int32_t* d_flag, void* stream);
+
 /* ------------------------------------------------------- grouped FP64 GEMM */
 /*
  * One problem: C[MxN] = alpha * op(A) * op(B) + beta * C, all row-major with

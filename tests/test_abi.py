@@ -82,6 +82,12 @@ int main(void) {
   F(FsOzProblem, N) F(FsOzProblem, K) F(FsOzProblem, a_rowtiles) F(FsOzProblem, b_rowtiles)
   F(FsOzProblem, ktiles) F(FsOzProblem, alpha) F(FsOzProblem, beta)
   S(FsOzTile) F(FsOzTile, problem) F(FsOzTile, tm) F(FsOzTile, tn)
+  S(FsSu2Group) F(FsSu2Group, u_off) F(FsSu2Group, ncols) F(FsSu2Group, dims)
+  F(FsSu2Group, divm) F(FsSu2Group, divs) F(FsSu2Group, ndim) F(FsSu2Group, M)
+  F(FsSu2Group, K) F(FsSu2Group, in_first) F(FsSu2Group, in_count)
+  F(FsSu2Group, out_first) F(FsSu2Group, out_count)
+  S(FsSu2Piece) F(FsSu2Piece, base) F(FsSu2Piece, sr_stride) F(FsSu2Piece, sc_stride)
+  F(FsSu2Piece, ext) F(FsSu2Piece, sr) F(FsSu2Piece, sc) F(FsSu2Piece, row0)
   S(FsOz2Operand) F(FsOz2Operand, src) F(FsOz2Operand, s_row) F(FsOz2Operand, s_k)
   F(FsOz2Operand, slices) F(FsOz2Operand, exps) F(FsOz2Operand, rows) F(FsOz2Operand, K)
   F(FsOz2Operand, rowtiles) F(FsOz2Operand, ktiles) F(FsOz2Operand, bits)
@@ -112,6 +118,8 @@ DTYPES = {
     "FsOzOperand": _native.OZ_OPERAND_DTYPE,
     "FsOzProblem": _native.OZ_PROBLEM_DTYPE,
     "FsOzTile": _native.OZ_TILE_DTYPE,
+    "FsSu2Group": _native.SU2_GROUP_DTYPE,
+    "FsSu2Piece": _native.SU2_PIECE_DTYPE,
     "FsOz2Operand": _native.OZ2_OPERAND_DTYPE,
     "FsOz2Problem": _native.OZ2_PROBLEM_DTYPE,
     "FsSplitReduce": _native.SPLIT_REDUCE_DTYPE,

@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 import torch
 
-from frostspin_b200.symmetric_tensor import su2_cg
+from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
+from frostspin_b200.symmetric_tensor import su2_cg, su2_fused_plan
 from frostspin_b200.symmetric_tensor.abelian_plan import emulate_permute
 from frostspin_b200.symmetric_tensor.su2_symmetric_tensor import (
     SU2SymmetricTensor,
@@ -42,6 +43,10 @@ def emulate_map(m, src):
         X = x[m.x_off[g] : m.x_off[g] + K * N].reshape(K, N)
         y[y_off[g] : y_off[g] + M * N] = (U @ X).ravel()
     out = emulate_permute(_Tables(m.scatter[0], m.out_size), y)
+    if getattr(m, "fused", None) is not None:
+        # the simple blocks the fused kernel takes, applied as it indexes them
+        su2_fused_plan.check(m.fused[0], m.fused[1], src.size, m.out_size, m.u_host.size)
+        su2_fused_plan.emulate(*m.fused, m.u_host, src, out)
     if m.zero_out:
         out = np.nan_to_num(out, nan=0.0)
     assert not np.isnan(out).any()
@@ -81,16 +86,27 @@ def permute_cases(d):
             i += 1
 
 
+@pytest.fixture(params=["fused", "three_launch"])
+def fused_mode(request):
+    """Permute maps built with the fused kernel for the thin simple blocks
+    (the default) and without it."""
+    lg.set_fused_permute(request.param == "fused")
+    yield request.param
+    lg.set_fused_permute(True)
+
+
 @pytest.mark.parametrize("trans", [False, True])
-def test_su2_permute_tables_match_reference(trans):
+def test_su2_permute_tables_match_reference(trans, fused_mode):
     d = load("su2")
     n = 0
+    n_fused = 0
     for base, i in permute_cases(d):
         t = host_tensor(d, base, trans=trans)
         pre = f"{base}_perm{i}"
         axes = tuple(int(a) for a in d[pre + "_axes"])
         nrr = int(d[pre + "_nrr"])
         m = t._permute_map(axes, nrr)
+        n_fused += m.fused is not None
         out = emulate_map(m, t.data.numpy())
         irr, blocks = ref_blocks(d, pre)
         assert np.array_equal(m.out_irreps, irr), pre
@@ -102,6 +118,7 @@ def test_su2_permute_tables_match_reference(trans):
             assert np.abs(got - b).max() <= TOL * scale, pre
         n += 1
     assert n >= 15
+    assert (n_fused > 0) == (fused_mode == "fused")
 
 
 def test_su2_dense_conversions_match_reference():
