@@ -175,18 +175,38 @@ def test_su2_cast_to_u1():
     assert abs(u.norm() - t.norm()) <= 1e-13 * t.norm()
 
 
-def test_su2_native_kernels_launched():
-    """The SU(2) permute runs through the C-ABI: gather, recoupling GEMM and
-    scatter launches are counted by the native layer."""
+@pytest.mark.parametrize("fused", [True, False])
+def test_su2_native_kernels_launched(fused):
+    """The SU(2) permute runs through the C-ABI: with the fused kernel (the
+    default) one launch takes the simple blocks with small recoupling
+    matrices; without it, gather, recoupling GEMM and scatter launches.  Both
+    give the reference's blocks."""
     from frostspin_b200 import _native
+    from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
 
     d = load("su2")
     t = su2_from(d, "r5")
-    before = dict(_native.CALL_COUNTS)
-    t.permute((3, 0, 2), (1, 4))
-    after = _native.CALL_COUNTS
-    assert after.get("fs_abelian_permute", 0) - before.get("fs_abelian_permute", 0) == 2
-    gemms = sum(after.get(k, 0) - before.get(k, 0)
-                for k in ("fs_grouped_dgemm", "fs_grouped_dgemm_uniform",
-                          "fs_grouped_dgemm_thin"))
-    assert 1 <= gemms <= 2  # thin groups and tiled groups, one launch each
+    lg.set_fused_permute(fused)
+    try:
+        before = dict(_native.CALL_COUNTS)
+        p = t.permute((3, 0, 2), (1, 4))
+        after = dict(_native.CALL_COUNTS)
+        lg.set_fused_permute(not fused)
+        q = t.permute((3, 0, 2), (1, 4))
+    finally:
+        lg.set_fused_permute(True)
+
+    def delta(*names):
+        return sum(after.get(k, 0) - before.get(k, 0) for k in names)
+
+    gemms = delta("fs_grouped_dgemm", "fs_grouped_dgemm_uniform", "fs_grouped_dgemm_thin")
+    if fused:
+        assert delta("fs_su2_permute_fused") == 1
+        # blocks beyond the fused kernel's limits, if any, take the other path
+        assert delta("fs_abelian_permute") in (0, 2)
+    else:
+        assert delta("fs_su2_permute_fused") == 0
+        assert delta("fs_abelian_permute") == 2
+        assert 1 <= gemms <= 2  # thin groups and tiled groups, one launch each
+    for a, b in zip(p.host_blocks(), q.host_blocks(), strict=True):
+        assert np.abs(a - b).max() <= TOL * max(1.0, np.abs(b).max())
