@@ -1042,6 +1042,105 @@ def run_simple_update(args, world, rank, local):
     }
 
 
+BATCH_RUNS = 64
+BATCH_CHIS = (16, 32, 64, 96)
+
+
+def batched_specs(seed=SEED):
+    """The 64 Z2 Ising runs of the batched workload: beta uniform in
+    [0.30, 0.60] and chi drawn from {16, 32, 64, 96} with a fixed seed."""
+    rng = np.random.default_rng(seed)
+    betas = rng.uniform(0.30, 0.60, BATCH_RUNS)
+    chis = rng.choice(BATCH_CHIS, BATCH_RUNS)
+    return [(float(b), int(c)) for b, c in zip(betas, chis, strict=True)]
+
+
+def run_batched(args, world, rank, local):
+    """Config 5 (its Z2 half): 64 independent C4v Ising CTMRG runs of uneven
+    chi advanced in lock step by iterate_c4v_many, each step one grouped GEMM
+    launch and one multi-buffer permute launch for all runs.  One step = one
+    iteration of every run; value = run-iterations per second."""
+    import torch
+
+    from frostspin_b200 import _native
+    from frostspin_b200.ctmrg import (energy_per_bond, ising_initial_environment,
+                                      ising_site_tensors, iterate_c4v_many)
+
+    specs = batched_specs()
+    runs = []
+    for i, (beta, chi) in enumerate(specs):
+        a, a2, a0d, mopd = ising_site_tensors(beta)
+        s, T = ising_initial_environment(chi, np.random.default_rng(42 + i))
+        runs.append([s, T, a, a2, chi, a0d, mopd])
+
+    def step():
+        res = iterate_c4v_many([r[:5] for r in runs])
+        for r, (s, T) in zip(runs, res, strict=True):
+            r[0], r[1] = s, T
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = _native.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = _native.kernel_launches() - n0
+    clk = clocks.stop()
+    t = max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, world)
+    energies = [energy_per_bond(r[0], r[1], r[5], r[6]) for r in runs[:4]]
+    line = {
+        "metric": "batched C4v CTMRG run-iterations/s (64 Z2 Ising runs, uneven chi)",
+        "value": world * BATCH_RUNS * args.steps / t, "unit": "run-iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded betas, chis and starting environments)", "impl": "ours",
+        "config": {"workload": "batched_ising_c4v", "runs": BATCH_RUNS,
+                   "beta_range": [0.30, 0.60], "chis": list(BATCH_CHIS),
+                   "chi_counts": {str(c): sum(1 for _, x in specs if x == c) for c in BATCH_CHIS},
+                   "energies_first_runs": energies,
+                   "u1_runs": "not built: the reference gives no U(1) classical C4v model",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_batched_sample()
+    return line
+
+
+def cpu_batched_sample():
+    """The oracle's C4v iteration of every run of the batched workload in a
+    sequential loop, one BLAS thread: one untimed and one timed pass."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import frostspin_oracle as fo
+
+    specs = batched_specs()
+    runs = []
+    for i, (beta, chi) in enumerate(specs):
+        a, a2, _, _ = fo.ising_tensors(beta)
+        sb, si, T = fo.ising_initial_env(chi, np.random.default_rng(42 + i))
+        runs.append([sb, si, T, a, a2, chi])
+    with threadpool_limits(limits=1):
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            for r in runs:
+                r[0], r[1], r[2] = fo.ising_c4v_iteration(r[0], r[1], r[2], r[3], r[4], r[5])
+            times.append(time.perf_counter() - t0)
+    t = times[-1]
+    return {"value": BATCH_RUNS / t, "unit": "run-iter/s", "cores": 1, "kind": "port",
+            "sample": f"numpy oracle C4v iteration of all {BATCH_RUNS} runs in a loop, one "
+                      f"pass after one warm-up pass: {t:.2f} s per pass"}
+
+
 def cpu_ising_sample(n):
     """The oracle's C4v iteration (numpy restatement of the reference example)
     from the same seeded start, one BLAS thread: mean time of n iterations
@@ -1069,6 +1168,18 @@ def run_reference(args, world, rank):
         return None
     if args.workload == "ctmrg":
         return run_reference_ctmrg(args, world)
+    if args.workload == "batched":
+        info = cpu_batched_sample()
+        v = info["value"]
+        return {"metric": "batched C4v CTMRG run-iterations/s (64 Z2 Ising runs, uneven chi)",
+                "value": v, "unit": "run-iter/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * BATCH_RUNS / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "batched_ising_c4v", "runs": BATCH_RUNS},
+                "cpu_baseline": info,
+                "e2e": {"value": v, "unit": "run-iter/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     if args.workload == "ising":
         info = cpu_ising_sample(max(args.steps, 20))
         v = info["value"]
@@ -1154,7 +1265,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["ctmrg", "u1_microbench", "gemm", "ising",
-                                           "simple_update"],
+                                           "simple_update", "batched"],
                     default="ctmrg")
     ap.add_argument("--gemm-n", type=int, default=4096, help="matrix size of the gemm workload")
     ap.add_argument("--gemm-shape", default=None, help="M,N,K of the gemm workload (else n,n,n)")
@@ -1212,6 +1323,8 @@ def main():
         line = run_ising(args, world, rank, local)
     elif args.workload == "simple_update":
         line = run_simple_update(args, world, rank, local)
+    elif args.workload == "batched":
+        line = run_batched(args, world, rank, local)
     else:
         line = run_ours(args, world, rank, local)
     if rank == 0:

@@ -34,6 +34,10 @@ PERM_EB_DTYPE = np.dtype(
     ]
 )
 
+PERM_BUFFERS_DTYPE = np.dtype(
+    [("in", "<u8"), ("in_len", "<i8"), ("out", "<u8"), ("out_len", "<i8")]
+)
+
 PERM_TASK_DTYPE = np.dtype(
     [("eb", "<i4"), ("start", "<u4"), ("count", "<u4"), ("pad", "<u4")]
 )
@@ -251,6 +255,7 @@ SIGNATURES = {
         ctypes.c_int,
         [_P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P],
     ),
+    "fs_abelian_permute_multi": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _P]),
     "fs_su2_fused_limits": (ctypes.c_int, [_P, _P, _P]),
     "fs_su2_permute_fused": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _I64,
                                             _P, _I64, _P, _P]),
@@ -324,7 +329,7 @@ CALL_COUNTS = {}
 
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
-    "fs_abelian_permute": 1, "fs_su2_permute_fused": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
+    "fs_abelian_permute": 1, "fs_abelian_permute_multi": 1, "fs_su2_permute_fused": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
     "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2,
     "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1, "fs_ozaki2_split": 2, "fs_ozaki2_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,

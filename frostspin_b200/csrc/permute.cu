@@ -26,10 +26,16 @@ constexpr int kPermMaxRows = 1024;   // rows per task (shared-memory row table)
 // times the innermost strides.  Consecutive threads write consecutive outputs
 // (coalesced stores) and read consecutive inputs whenever the source keeps the
 // same innermost leg; each thread keeps kPermUnroll loads in flight.
+//
+// kMulti: the EBs of several independent permutes in one launch; EB e reads
+// and writes the buffer pair bufs[e.pad] (the permutes of many CTMRG runs
+// advanced in lock step share one launch).
+template <bool kMulti>
 __global__ void __launch_bounds__(kPermThreads, 4)
-    k_perm_gather(const double* __restrict__ in, int64_t in_len, double* __restrict__ out,
-                  int64_t out_len, const FsPermEB* __restrict__ ebs, int64_t n_ebs,
-                  const FsPermTask* __restrict__ tasks, int64_t n_tasks, int32_t* flag) {
+    k_perm_gather_t(const double* __restrict__ in0, int64_t in_len0, double* __restrict__ out0,
+                    int64_t out_len0, const FsPermBuffers* __restrict__ bufs, int64_t n_bufs,
+                    const FsPermEB* __restrict__ ebs, int64_t n_ebs,
+                    const FsPermTask* __restrict__ tasks, int64_t n_tasks, int32_t* flag) {
     __shared__ FsPermEB e;
     __shared__ int64_t row_src[kPermMaxRows];
     __shared__ int64_t row_dst[kPermMaxRows];
@@ -51,6 +57,20 @@ __global__ void __launch_bounds__(kPermThreads, 4)
         if (nd < 1 || nd > FS_PERM_MAXR) {
             if (threadIdx.x == 0) raise_flag(flag, FS_ERR_UNSUPPORTED);
             continue;
+        }
+        const double* in = in0;
+        double* out = out0;
+        int64_t in_len = in_len0, out_len = out_len0;
+        if (kMulti) {
+            if (e.pad < 0 || e.pad >= n_bufs) {
+                if (threadIdx.x == 0) raise_flag(flag, FS_ERR_BOUNDS);
+                continue;
+            }
+            const FsPermBuffers b = bufs[e.pad];
+            in = b.in;
+            out = b.out;
+            in_len = b.in_len;
+            out_len = b.out_len;
         }
         const uint32_t L = e.dims[nd - 1];
         const int64_t osL = e.ostride[nd - 1];
@@ -120,7 +140,21 @@ extern "C" int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_
     // one wave of resident CTAs (4 per SM at the kernel's register budget)
     const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 4;
     const int grid = static_cast<int>(n_tasks < max_grid ? n_tasks : max_grid);
-    fsb::k_perm_gather<<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
-        d_in, in_len, d_out, out_len, d_ebs, n_ebs, d_tasks, n_tasks, d_flag);
+    fsb::k_perm_gather_t<false><<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
+        d_in, in_len, d_out, out_len, nullptr, 0, d_ebs, n_ebs, d_tasks, n_tasks, d_flag);
+    return fsb::launch_status();
+}
+
+extern "C" int fs_abelian_permute_multi(const FsPermBuffers* d_bufs, int64_t n_bufs,
+                                        const FsPermEB* d_ebs, int64_t n_ebs,
+                                        const FsPermTask* d_tasks, int64_t n_tasks,
+                                        int32_t* d_flag, void* stream) {
+    if (n_tasks < 0 || n_ebs < 0 || n_bufs < 0) return FS_ERR_INVALID_ARG;
+    if (n_tasks == 0) return FS_OK;
+    if (d_bufs == nullptr || d_ebs == nullptr || d_tasks == nullptr) return FS_ERR_INVALID_ARG;
+    const int64_t max_grid = static_cast<int64_t>(fsb::num_sms()) * 4;
+    const int grid = static_cast<int>(n_tasks < max_grid ? n_tasks : max_grid);
+    fsb::k_perm_gather_t<true><<<grid, fsb::kPermThreads, 0, fsb::as_stream(stream)>>>(
+        nullptr, 0, nullptr, 0, d_bufs, n_bufs, d_ebs, n_ebs, d_tasks, n_tasks, d_flag);
     return fsb::launch_status();
 }

@@ -7,6 +7,7 @@ from .classical_c4v import (
     ising_initial_environment,
     ising_site_tensors,
     iterate_c4v,
+    iterate_c4v_many,
 )
 from .ctm_environment import CTMEnvironment
 from .sequential_ctmrg import SequentialCTMRG
@@ -26,4 +27,5 @@ __all__ = [
     "ising_initial_environment",
     "ising_site_tensors",
     "iterate_c4v",
+    "iterate_c4v_many",
 ]

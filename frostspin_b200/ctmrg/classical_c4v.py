@@ -34,6 +34,48 @@ def iterate_c4v(s, T, a, a2, chi_target):
     return news, newT
 
 
+def iterate_c4v_many(runs):
+    """One iteration of many independent C4v runs advanced in lock step:
+    runs is a list of (s, T, a, a2, chi_target); returns [(s, T)].  Each run
+    does exactly what iterate_c4v does (examples/ising_classical_ctmrg.py
+    :115-204), but every step issues its sector GEMMs of all runs as one
+    grouped launch and its permutes of all runs as one multi-buffer launch
+    (linalg.shared_launches), and the corner eigendecompositions of all runs
+    are batched by block size."""
+    from .. import linalg
+    from ..symmetric_tensor.symmetric_tensor import SymmetricTensor
+
+    def each(fn, *lists):
+        with linalg.shared_launches():
+            return [fn(*xs) for xs in zip(*lists, strict=True)]
+
+    ss = [r[0] for r in runs]
+    Ts = [r[1] for r in runs]
+    As = [r[2] for r in runs]
+    A2s = [r[3] for r in runs]
+    chis = [r[4] for r in runs]
+    Tp = each(lambda T: T.permute((0, 1), (2,)), Ts)
+    mat = [t * s for t, s in zip(Tp, ss, strict=True)]
+    mat = each(lambda m, T: m @ T, mat, Ts)
+    mat = each(lambda m: m.permute((1, 2), (0, 3)), mat)
+    mat = each(lambda a2, m: a2 @ m, A2s, mat)
+    mat = each(lambda m: m.permute((0, 2), (1, 3)), mat)
+    eig = SymmetricTensor.truncated_eigh_many(mat, chis)
+    news = [s for s, _ in eig]
+    Us = [u for _, u in eig]
+    for s in news:
+        s /= s.norm_device()
+    nT = each(lambda U: U.permute((1,), (0, 2)), Us)
+    nT = each(lambda tp, t: tp @ t, Tp, nT)
+    nT = each(lambda t: t.permute((1, 2), (0, 3)), nT)
+    nT = each(lambda a, t: a @ t, As, nT)
+    nT = each(lambda t: t.permute((0, 2), (1, 3)), nT)
+    nT = each(lambda U, t: U.dagger() @ t, Us, nT)
+    for t in nT:
+        t /= t.norm_device()
+    return list(zip(news, nT, strict=True))
+
+
 def env_1site(s, T):
     """examples/ising_classical_ctmrg.py:207-251."""
     Tp = T.permute((0, 1), (2,))

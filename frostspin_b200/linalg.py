@@ -92,6 +92,68 @@ def ozaki_pair_mode(enabled):
 # autotuner and the profiling scripts replay)
 _RECORDER = None
 
+# when a dict: grouped GEMM problems and abelian permutes are collected and
+# launched together when the shared_launches block ends
+_SHARED = None
+
+
+@contextlib.contextmanager
+def shared_launches():
+    """Collect the sector GEMMs and abelian permutes issued inside the block
+    and launch them together on exit: one grouped GEMM launch for all GEMM
+    problems and one multi-buffer permute launch for all permutes.  The
+    operations inside must be independent of each other (one step of many
+    independent runs); their output buffers exist as soon as the call
+    returns, their contents once the block has ended."""
+    global _SHARED
+    old, _SHARED = _SHARED, {"gemm": [], "perm": []}
+    try:
+        yield
+        pend = _SHARED
+        _SHARED = old
+        if pend["perm"]:
+            _flush_permutes(pend["perm"])
+        if pend["gemm"]:
+            grouped_gemm(pend["gemm"])
+    finally:
+        _SHARED = old
+
+
+def defer_permute(ebs, tasks, src, out, nbytes):
+    """Queue one abelian permute (its host EB and task tables, source and
+    destination buffers) for the enclosing shared_launches block; returns
+    False when no block is open."""
+    if _SHARED is None:
+        return False
+    _SHARED["perm"].append((ebs, tasks, src, out, nbytes))
+    return True
+
+
+def _flush_permutes(items):
+    bufs = np.zeros(len(items), dtype=_native.PERM_BUFFERS_DTYPE)
+    ebs_all, tasks_all = [], []
+    n_eb = 0
+    nbytes = 0.0
+    for i, (ebs, tasks, src, out, nb) in enumerate(items):
+        bufs[i] = (dev.ptr(src), int(src.numel()), dev.ptr(out), int(out.numel()))
+        e = ebs.copy()
+        e["pad"] = i
+        t = tasks.copy()
+        t["eb"] += n_eb
+        n_eb += e.size
+        ebs_all.append(e)
+        tasks_all.append(t)
+        nbytes += nb
+    ebs_all = np.concatenate(ebs_all)
+    tasks_all = np.concatenate(tasks_all)
+    if tasks_all.size == 0:
+        return
+    d_bufs, d_ebs, d_tasks = dev.upload(bufs), dev.upload(ebs_all), dev.upload(tasks_all)
+    with instrument.region("permute", bytes=nbytes):
+        _native.call("fs_abelian_permute_multi", d_bufs.data_ptr(), bufs.size,
+                     d_ebs.data_ptr(), ebs_all.size, d_tasks.data_ptr(), tasks_all.size,
+                     None, dev.stream())
+
 
 @contextlib.contextmanager
 def record_gemm_calls():
@@ -123,6 +185,9 @@ def grouped_gemm(problems):
     """
     n = len(problems)
     if n == 0:
+        return
+    if _SHARED is not None:
+        _SHARED["gemm"].extend(problems)
         return
     arr = np.zeros(n, dtype=_native.GEMM_PROBLEM_DTYPE)
     tm, tn = _tile_shape()

@@ -11,9 +11,8 @@ from collections import OrderedDict
 import numpy as np
 import torch
 
-from .. import _native
+from .. import _native, instrument, linalg
 from .. import device as dev
-from .. import instrument
 from .abelian_plan import (
     GroupInfo,
     build_abelian_permute_plan,
@@ -184,6 +183,9 @@ class AbelianSymmetricTensor(SymmetricTensor):
         """abelian_symmetric_tensor.py:395-430 on the device."""
         plan = self._permute_plan(axes, nrr)
         out = dev.empty_f64(plan.size)
+        if plan.size and linalg.defer_permute(plan.ebs, plan.tasks, self._data, out,
+                                              16.0 * plan.size):
+            return out, plan.offsets, plan.block_shapes, plan.block_irreps
         if plan.size:
             if plan.device_tables is None:
                 plan.device_tables = (dev.upload(plan.ebs), dev.upload(plan.tasks))

@@ -779,6 +779,53 @@ class SymmetricTensor:
             return s, u
         return s
 
+    @staticmethod
+    def truncated_eigh_many(tensors, nvals, *, atol=0.0, rtol=None, degen_ratio=1.0):
+        """truncated_eigh of many independent tensors (the corners of many
+        CTMRG runs advanced in lock step): every block of every tensor is
+        diagonalised with the other blocks of the same size in one batched
+        cuSOLVER call, the kept eigenvalues of all tensors come to the host in
+        one copy, then each tensor is truncated as truncated_eigh does.
+        Returns [(s, u)] in the order of `tensors`."""
+        jobs = []
+        per = []
+        for ti, (t, nv) in enumerate(zip(tensors, nvals, strict=True)):
+            if not t.is_square_matrix():
+                raise ValueError("Tensor legs do not define a square matrix")
+            irreps, shapes = t.get_block_sizes(t._row_reps, t._col_reps, t._signature)
+            nb = len(shapes)
+            lookup = {t._irrep_key(q): i for i, q in enumerate(t._block_irreps)}
+            dims = np.array([t.irrep_dimension(irreps[bi]) for bi in range(nb)], dtype=np.int64)
+            per.append((irreps, dims, [None] * nb, [None] * nb, [np.zeros((1,))] * nb))
+            for bi in range(nb):
+                j = lookup.get(t._irrep_key(irreps[bi]))
+                if j is not None:
+                    jobs.append((ti, bi, t.blocks[j], int(nv // dims[bi] + 1)))
+        by_shape = {}
+        for job in jobs:
+            by_shape.setdefault(tuple(job[2].shape), []).append(job)
+        pending = []
+        for group in by_shape.values():
+            w, v = torch.linalg.eigh(torch.stack([job[2] for job in group]))
+            for gi, (ti, bi, _, k) in enumerate(group):
+                a = torch.abs(w[gi])
+                so = torch.argsort(a, descending=True, stable=True)[: min(k, a.numel())]
+                per[ti][2][bi] = w[gi][so]
+                per[ti][3][bi] = v[gi][:, so]
+                pending.append((ti, bi, a[so]))
+        host = torch.cat([a for _, _, a in pending]).cpu().numpy() if pending else None
+        pos = 0
+        for ti, bi, a in pending:
+            per[ti][4][bi] = host[pos: pos + a.numel()]
+            pos += a.numel()
+        out = []
+        for t, nv, (irreps, dims, vals, vecs, absv) in zip(tensors, nvals, per, strict=True):
+            cuts = find_block_cuts(absv, nv, dims=dims, atol=atol, rtol=rtol,
+                                   degen_ratio=degen_ratio)
+            u, sv, _ = t._truncate(vals, irreps, cuts, vecs)
+            out.append((sv, u))
+        return out
+
     @classmethod
     def eigs(cls, matmat, nvals, reps, signature, *, atol=0.0, rtol=None, degen_ratio=1.0,
              dmax_full=100, compute_vectors=False, rng=None, maxiter=4000, arpack_tol=0):

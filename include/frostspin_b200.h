@@ -81,7 +81,7 @@ typedef struct FsPermEB {
     uint32_t volume;                 /* product of dims, < 2^31                 */
     int32_t tile_leg;                /* leg with ostride == 1 for a tiled
                                         transpose, -1 for a plain gather        */
-    int32_t pad;
+    int32_t pad;                     /* fs_abelian_permute_multi: buffer pair   */
 } FsPermEB;
 
 typedef struct FsPermTask {
@@ -155,6 +155,24 @@ int fs_su2_permute_fused(const double* d_src, int64_t src_len, double* d_out, in
                          const FsSu2Piece* d_pieces, int64_t n_pieces, const double* d_u,
                          int64_t u_len, const FsPermTask* d_tasks, int64_t n_tasks,
                          int32_t* d_flag, void* stream);
+
+/*
+ * Several independent abelian permutes in one launch (the permutes of many
+ * CTMRG runs advanced in lock step; the reference runs them one by one through
+ * AbelianSymmetricTensor._permute_data, abelian_symmetric_tensor.py:395-430).
+ * Same EB and task tables as fs_abelian_permute, concatenated; the pad field
+ * of every EB indexes the buffer pair it reads and writes in d_bufs.
+ */
+typedef struct FsPermBuffers {
+    const double* in;
+    int64_t in_len;
+    double* out;
+    int64_t out_len;
+} FsPermBuffers;
+
+int fs_abelian_permute_multi(const FsPermBuffers* d_bufs, int64_t n_bufs,
+                             const FsPermEB* d_ebs, int64_t n_ebs, const FsPermTask* d_tasks,
+                             int64_t n_tasks, int32_t* d_flag, void* stream);
 
 /* ------------------------------------------------------- grouped FP64 GEMM */
 /*

@@ -62,6 +62,8 @@ int main(void) {
   F(FsPermEB, nstride) F(FsPermEB, dims) F(FsPermEB, divm) F(FsPermEB, divs)
   F(FsPermEB, ndim) F(FsPermEB, volume) F(FsPermEB, tile_leg)
   S(FsPermTask) F(FsPermTask, eb) F(FsPermTask, start) F(FsPermTask, count)
+  S(FsPermBuffers) F(FsPermBuffers, in) F(FsPermBuffers, in_len) F(FsPermBuffers, out)
+  F(FsPermBuffers, out_len)
   S(FsGemmProblem) F(FsGemmProblem, A) F(FsGemmProblem, B) F(FsGemmProblem, C)
   F(FsGemmProblem, lda) F(FsGemmProblem, ldb) F(FsGemmProblem, ldc)
   F(FsGemmProblem, M) F(FsGemmProblem, N) F(FsGemmProblem, K)
@@ -110,6 +112,7 @@ int main(void) {
 DTYPES = {
     "FsPermEB": _native.PERM_EB_DTYPE,
     "FsPermTask": _native.PERM_TASK_DTYPE,
+    "FsPermBuffers": _native.PERM_BUFFERS_DTYPE,
     "FsGemmProblem": _native.GEMM_PROBLEM_DTYPE,
     "FsGemmTile": _native.GEMM_TILE_DTYPE,
     "FsSegment": _native.SEGMENT_DTYPE,
