@@ -1042,6 +1042,69 @@ def run_simple_update(args, world, rank, local):
     }
 
 
+def run_deviation(args, world, rank, local):
+    """Accuracy of the mixed path over a long run: from the same warmed-up
+    chi = 256 environment, plain FP64 and the mixed precision iterate side by
+    side; after each iteration count in --deviation the energies per bond are
+    compared and the truncation decisions (chi after every move) checked for
+    equality; at the end the horizontal correlation lengths are compared."""
+    import torch
+
+    from frostspin_b200 import autotune, linalg
+
+    mixed = args.precision if args.precision != "fp64" else "ozaki2_13"
+    points = sorted(int(x) for x in args.deviation.split(","))
+    su, tensors, ctm, _ = ctmrg_setup(args)
+    linalg.set_gemm_precision("fp64")
+    for w in range(args.warmup):
+        if w == args.warmup - 1 and args.autotune == "on":
+            with linalg.record_gemm_calls() as records:
+                ctm.iterate()
+        else:
+            ctm.iterate()
+    if args.autotune == "on":
+        autotune.tune(records, mixed)
+        autotune.set_enabled(True)
+    mix = ctm.copy()
+    rows = []
+    same_chi = True
+    t0 = time.perf_counter()
+    for it in range(1, points[-1] + 1):
+        linalg.set_gemm_precision("fp64")
+        ctm.iterate()
+        linalg.set_gemm_precision(mixed)
+        mix.iterate()
+        same_chi = same_chi and list(ctm.chi_values) == list(mix.chi_values)
+        if it in points:
+            linalg.set_gemm_precision("fp64")
+            e64 = energy_per_bond(ctm)
+            linalg.set_gemm_precision(mixed)
+            emx = energy_per_bond(mix)
+            rows.append({"iterations": it, "energy_fp64": e64, "energy_mixed": emx,
+                         "rel_err": abs(emx - e64) / abs(e64),
+                         "chi_decisions_identical": same_chi,
+                         "elapsed_s": time.perf_counter() - t0})
+            print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    linalg.check_ozaki_flags()
+    xi = None
+    if args.deviation_xi == "on":
+        linalg.set_gemm_precision("fp64")
+        x64 = ctm.compute_corr_length_h(0)
+        linalg.set_gemm_precision(mixed)
+        xmx = mix.compute_corr_length_h(0)
+        xi = {"xi_fp64": x64, "xi_mixed": xmx, "rel_err": abs(xmx - x64) / abs(x64)}
+    torch.cuda.synchronize()
+    return {"metric": "relative energy deviation, mixed vs plain FP64 CTMRG",
+            "value": rows[-1]["rel_err"], "unit": "relative", "n_gpus": world,
+            "steps": points[-1], "warmup": args.warmup, "higher_is_better": False,
+            "impl": "ours", "dtype": f"f64 via int8 {mixed}",
+            "config": {"workload": f"ctmrg_heisenberg_{args.symmetry}", "chi": args.chi,
+                       "D_target": args.D, "beta": args.beta, "precision": mixed,
+                       "points": rows, "correlation_length_h0": xi,
+                       "chi_values_fp64": [int(c) for c in ctm.chi_values],
+                       "chi_values_mixed": [int(c) for c in mix.chi_values]}}
+
+
 BATCH_RUNS = 64
 BATCH_CHIS = (16, 32, 64, 96)
 
@@ -1278,6 +1341,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fused-permute", choices=["on", "off"], default="on",
                     help="thin SU(2) simple blocks in the one-pass fused permute kernel")
+    ap.add_argument("--deviation", default="",
+                    help="iteration counts (e.g. 10,25,50) at which a side-by-side FP64 and "
+                         "mixed CTMRG run compares energies (accuracy study, not a bench line)")
+    ap.add_argument("--deviation-xi", choices=["on", "off"], default="on")
     ap.add_argument("--autotune", choices=["on", "off"], default="on",
                     help="measure the sector-GEMM shape classes of a warm-up iteration on "
                          "both paths and dispatch by the measurement")
@@ -1315,7 +1382,9 @@ def main():
     from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor
 
     lie_group_symmetric_tensor.set_fused_permute(args.fused_permute == "on")
-    if args.workload == "ctmrg":
+    if args.workload == "ctmrg" and args.deviation:
+        line = run_deviation(args, world, rank, local)
+    elif args.workload == "ctmrg":
         line = run_ctmrg(args, world, rank, local)
     elif args.workload == "gemm":
         line = run_gemm(args, world, rank, local)
