@@ -1339,7 +1339,7 @@ def main():
                     help="CTMRG corner dimension target (default 64 for U(1), 256 for SU(2))")
     ap.add_argument("--beta", type=float, default=2.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--fused-permute", choices=["on", "off"], default="on",
+    ap.add_argument("--fused-permute", choices=["on", "off"], default="off",
                     help="thin SU(2) simple blocks in the one-pass fused permute kernel")
     ap.add_argument("--deviation", default="",
                     help="iteration counts (e.g. 10,25,50) at which a side-by-side FP64 and "

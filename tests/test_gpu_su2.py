@@ -177,10 +177,10 @@ def test_su2_cast_to_u1():
 
 @pytest.mark.parametrize("fused", [True, False])
 def test_su2_native_kernels_launched(fused):
-    """The SU(2) permute runs through the C-ABI: with the fused kernel (the
-    default) one launch takes the simple blocks with small recoupling
-    matrices; without it, gather, recoupling GEMM and scatter launches.  Both
-    give the reference's blocks."""
+    """The SU(2) permute runs through the C-ABI: with the fused kernel one
+    launch takes the simple blocks with small recoupling matrices; without it
+    (the default), gather, recoupling GEMM and scatter launches.  Both give
+    the reference's blocks."""
     from frostspin_b200 import _native
     from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
 
@@ -194,7 +194,7 @@ def test_su2_native_kernels_launched(fused):
         lg.set_fused_permute(not fused)
         q = t.permute((3, 0, 2), (1, 4))
     finally:
-        lg.set_fused_permute(True)
+        lg.set_fused_permute(False)
 
     def delta(*names):
         return sum(after.get(k, 0) - before.get(k, 0) for k in names)

@@ -89,10 +89,10 @@ def permute_cases(d):
 @pytest.fixture(params=["fused", "three_launch"])
 def fused_mode(request):
     """Permute maps built with the fused kernel for the thin simple blocks
-    (the default) and without it."""
+    and without it (the default)."""
     lg.set_fused_permute(request.param == "fused")
     yield request.param
-    lg.set_fused_permute(True)
+    lg.set_fused_permute(False)
 
 
 @pytest.mark.parametrize("trans", [False, True])
