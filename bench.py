@@ -13,8 +13,9 @@ symmetry, D = 24 (whole multiplets: Dmax = 28), chi = 256.  `--symmetry u1`
 runs the same chain with U(1) sectors (defaults D = 12, chi = 64).  One step =
 one CTMRG iteration (up, right, down, left moves).  The timed iterations start
 from an environment warmed up for W iterations; the headline arithmetic
-(`--precision`, default ozaki7: sector GEMMs on the tcgen05 int8 tensor cores
-with 7 digit slices) runs exactly K iterations, the plain FP64 run (DMMA
+(`--precision`, default ozaki2_13: sector GEMMs on the tcgen05 int8 tensor
+cores, one product per modulus for 13 moduli, CRT in FP64; the autotuner picks
+the int8 or FP64 path per sector shape class) runs exactly K iterations, the plain FP64 run (DMMA
 tensor cores) min(K, 3) iterations from a copy of the same environment, and the
 energies per bond after the same number of iterations are compared.
 
@@ -369,7 +370,7 @@ def run_ctmrg(args, world, rank, local):
 
     from frostspin_b200 import linalg
 
-    mixed = args.precision if args.precision != "fp64" else "ozaki7"
+    mixed = args.precision if args.precision != "fp64" else "ozaki2_13"
     su, tensors, ctm, t_su = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
     for w in range(args.warmup):
@@ -1354,7 +1355,7 @@ def main():
                     help="chi values the CPU reference arm of the ctmrg workload measures")
     ap.add_argument("--ozaki-pair", choices=["on", "off"], default="on",
                     help="large int8 sector GEMMs on CTA pairs (tcgen05 cta_group::2)")
-    ap.add_argument("--precision", default="ozaki7",
+    ap.add_argument("--precision", default="ozaki2_13",
                     help="sector GEMM arithmetic: fp64, ozakiS (S = 3..8 int8 digit slices) "
                          "or ozaki2_N (N = 8..14 int8 moduli, CRT)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,
