@@ -20,12 +20,14 @@ def truncated_svd_block(m, k, *, full, n_iter=3, oversampling=None):
     X^H X plays in the reference's sparse_svd (svd_tools.py:154-197), with the
     products on the device.  Returns (U, s, Vh) with s decreasing.
     """
+    from .. import instrument, linalg
+
     nr, nc = m.shape
     dmin = min(nr, nc)
     if full or k >= dmin // 2:
-        u, s, vh = torch.linalg.svd(m, full_matrices=False)
+        with instrument.region("svd_dense", elems=float(nr * nc)):
+            u, s, vh = torch.linalg.svd(m, full_matrices=False)
         return u, s, vh
-    from .. import linalg
 
     p = k + 10 if oversampling is None else oversampling
     kk = min(dmin, k + p)
@@ -33,14 +35,18 @@ def truncated_svd_block(m, k, *, full, n_iter=3, oversampling=None):
     g.manual_seed(1234 + nr * 7 + nc)
     omega = torch.randn(nc, kk, dtype=m.dtype, device=m.device, generator=g)
     _, _, _, (y,) = linalg.matmul_blocks([m], [omega])
-    q, _ = torch.linalg.qr(y, mode="reduced")
+    with instrument.region("svd_qr"):
+        q, _ = torch.linalg.qr(y, mode="reduced")
     for _ in range(n_iter):
         _, _, _, (z,) = linalg.matmul_blocks([m.T], [q])
-        z, _ = torch.linalg.qr(z, mode="reduced")
+        with instrument.region("svd_qr"):
+            z, _ = torch.linalg.qr(z, mode="reduced")
         _, _, _, (y,) = linalg.matmul_blocks([m], [z])
-        q, _ = torch.linalg.qr(y, mode="reduced")
+        with instrument.region("svd_qr"):
+            q, _ = torch.linalg.qr(y, mode="reduced")
     _, _, _, (b,) = linalg.matmul_blocks([q.T], [m])
-    ub, s, vh = torch.linalg.svd(b, full_matrices=False)
+    with instrument.region("svd_small"):
+        ub, s, vh = torch.linalg.svd(b, full_matrices=False)
     _, _, _, (u,) = linalg.matmul_blocks([q], [ub])
     return u[:, :k], s[:k], vh[:k]
 

@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 from .. import device as dev
+from .. import instrument
 from .. import linalg
 from ..misc_tools.svd_tools import find_block_cuts
 from .diagonal_tensor import DiagonalTensor
@@ -764,7 +765,8 @@ class SymmetricTensor:
             j = lookup.get(self._irrep_key(irreps[bi]))
             if j is None:
                 continue
-            w, v = torch.linalg.eigh(self.blocks[j])
+            with instrument.region("eigh"):
+                w, v = torch.linalg.eigh(self.blocks[j])
             a = torch.abs(w)
             so = torch.argsort(a, descending=True, stable=True)[: min(k, a.numel())]
             vals[bi] = w[so]
