@@ -44,6 +44,12 @@ import time
 
 import numpy as np
 
+# The chi = 256 working set is many sector buffers of very uneven sizes (tens of
+# KB to ~11 GB) allocated and freed every move; with fixed segments the caching
+# allocator fragments until a request of ~11 GB fails with ~100 GB reserved but
+# unused.  Growable segments keep the reserved memory reusable.
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -400,26 +406,35 @@ def run_ctmrg(args, world, rank, local):
     n_cmp = min(args.steps, 3)
     n64 = args.steps if not headline_mixed else n_cmp
     nmx = args.steps if headline_mixed else n_cmp
+    # energies after the same number of iterations from the same start; each
+    # environment is dropped as soon as its energy is known (four chi = 256
+    # environments plus the rdm intermediates do not fit at once)
     barrier(world)
     t64, clk64, k64, l64 = timed_iterations(ctm, n64, "fp64", local)
+    chi_values = [int(c) for c in ctm.chi_values]
+    e64 = energy_per_bond(ctm) if n64 == n_cmp else None
+    del ctm
+    torch.cuda.empty_cache()
     ctm_mixed = start_env.copy()
     barrier(world)
     tmx, clkmx, kmx, lmx = timed_iterations(ctm_mixed, nmx, mixed, local)
-    # energies after the same number of iterations from the same start
-    ref_env = ctm if n64 == n_cmp else None
-    mix_env = ctm_mixed if nmx == n_cmp else None
-    if ref_env is None:
-        ref_env = start_env.copy()
-        linalg.set_gemm_precision("fp64")
+    emx = energy_per_bond(ctm_mixed) if nmx == n_cmp else None
+    if args.symmetry != "u1":
+        del ctm_mixed
+    torch.cuda.empty_cache()
+    for prec in ("fp64", mixed):
+        if (e64 if prec == "fp64" else emx) is not None:
+            continue
+        env = start_env.copy()
+        linalg.set_gemm_precision(prec)
         for _ in range(n_cmp):
-            ref_env.iterate()
-    if mix_env is None:
-        mix_env = start_env.copy()
-        linalg.set_gemm_precision(mixed)
-        for _ in range(n_cmp):
-            mix_env.iterate()
-    e64 = energy_per_bond(ref_env)
-    emx = energy_per_bond(mix_env)
+            env.iterate()
+        if prec == "fp64":
+            e64 = energy_per_bond(env)
+        else:
+            emx = energy_per_bond(env)
+        del env
+        torch.cuda.empty_cache()
     t64 = max_over_ranks(t64, world)
     tmx = max_over_ranks(tmx, world)
     t_head = tmx if headline_mixed else t64
@@ -444,6 +459,8 @@ def run_ctmrg(args, world, rank, local):
     ee.record()
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
+    del e2e_env, new
+    torch.cuda.empty_cache()
     h2d = int(sum(h.numel() * 8 for h in hostA))
     d2h = int(4 * 2 * 16 * 8)  # four 2x2x2x2 reduced density matrices per site pair
 
@@ -516,7 +533,7 @@ def run_ctmrg(args, world, rank, local):
             "model": ("spin-1/2 Heisenberg square lattice, AB/BA cell, "
                       + ("SU(2) multiplets" if args.symmetry == "su2" else "U(1) sectors")),
             "beta": args.beta, "D_target": args.D, "Dmax": su.Dmax, "chi": args.chi,
-            "chi_values": [int(c) for c in ctm.chi_values],
+            "chi_values": chi_values,
             "precision": mixed if headline_mixed else "fp64",
             "ozaki_pair": args.ozaki_pair,
             "autotune": tune_info,

@@ -4,10 +4,20 @@ PyTorch only provides memory, streams and host<->device copies here; every
 computation on symmetric-tensor data goes through the C ABI in ``_native``.
 """
 
-import numpy as np
-import torch
+import os
 
-from . import _native
+# Sector buffers range from tens of KB to ~11 GB (chi = 256 SU(2) CTMRG) and are
+# allocated and freed every move; with the caching allocator's fixed segments
+# that pattern fragments until a large request fails with most of the reserved
+# memory unused.  Growable segments are the default here unless the process
+# configured the allocator itself; the setting only takes effect when this
+# module is imported before torch's first CUDA allocation.
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+from . import _native  # noqa: E402
 
 _scratch = {}
 _available = []
