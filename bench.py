@@ -357,18 +357,27 @@ def timed_iterations(ctm, steps, precision, local):
     e = torch.cuda.Event(enable_timing=True)
     # NVTX range for profilers: "timed_fp64" or "timed_mixed"
     torch.cuda.nvtx.range_push("timed_fp64" if precision == "fp64" else "timed_mixed")
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     s.record()
-    for _ in range(steps):
+    for i in range(steps):
         ctm.iterate()
+        marks[i].record()
     e.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     clk = clocks.stop()
     instrument.disable()
     kernels = instrument.summary()
+    kernels["per_iteration_s"] = [round(a.elapsed_time(b) * 1e-3, 4)
+                                  for a, b in zip([s, *marks[:-1]], marks, strict=True)]
     launches = _native.kernel_launches() - n0
     linalg.check_ozaki_flags()
     return s.elapsed_time(e) * 1e-3, clk, kernels, launches
+
+
+def _kernel_table(kern):
+    return {k: (v if k == "per_iteration_s" else {kk: round(vv, 4) for kk, vv in v.items()})
+            for k, v in kern.items()}
 
 
 def run_ctmrg(args, world, rank, local):
@@ -379,12 +388,14 @@ def run_ctmrg(args, world, rank, local):
     mixed = args.precision if args.precision != "fp64" else "ozaki2_13"
     su, tensors, ctm, t_su = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
-    for w in range(args.warmup):
-        if w == args.warmup - 1 and args.autotune == "on":
-            # the last warm-up iteration records the sector GEMM launches; the
-            # tuner measures their shape classes on both paths before timing
-            with linalg.record_gemm_calls() as records:
+    # the warm-up iterations record the sector GEMM launches; the tuner
+    # measures their shape classes on both paths before timing
+    records = []
+    for _ in range(args.warmup):
+        if args.autotune == "on":
+            with linalg.record_gemm_calls() as rec:
                 ctm.iterate()
+            records += rec
         else:
             ctm.iterate()
     torch.cuda.synchronize()
@@ -543,8 +554,8 @@ def run_ctmrg(args, world, rank, local):
             "energy_iterations_compared": n_cmp,
             "energy_fp64": e64, "energy_mixed": emx,
             "energy_rel_err_mixed_vs_fp64": abs(emx - e64) / abs(e64),
-            "kernels_fp64_run": {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in k64.items()},
-            "kernels_mixed_run": {k: {kk: round(vv, 4) for kk, vv in v.items()} for k, v in kmx.items()},
+            "kernels_fp64_run": _kernel_table(k64),
+            "kernels_mixed_run": _kernel_table(kmx),
             "simple_update_setup_s": t_su,
             "l2": "working set > 126 MB L2 (no flush needed)",
             "parallelism": f"replicas x{world}",
@@ -1074,10 +1085,12 @@ def run_deviation(args, world, rank, local):
     points = sorted(int(x) for x in args.deviation.split(","))
     su, tensors, ctm, _ = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
-    for w in range(args.warmup):
-        if w == args.warmup - 1 and args.autotune == "on":
-            with linalg.record_gemm_calls() as records:
+    records = []
+    for _ in range(args.warmup):
+        if args.autotune == "on":
+            with linalg.record_gemm_calls() as rec:
                 ctm.iterate()
+            records += rec
         else:
             ctm.iterate()
     if args.autotune == "on":

@@ -98,6 +98,8 @@ GEMM_TILE_DTYPE = np.dtype(
     [("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")]
 )
 
+TILE_RUN_DTYPE = np.dtype([("start", "<i8"), ("problem", "<i4"), ("ncol", "<i4")])
+
 SPLIT_REDUCE_DTYPE = np.dtype(
     [
         ("W", "<u8"),
@@ -265,6 +267,7 @@ SIGNATURES = {
     "fs_grouped_dgemm_thin": (ctypes.c_int, [_P, _I64, _P, _I64, _P]),
     "fs_grouped_dgemm_uniform": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P]),
     "fs_splitk_reduce": (ctypes.c_int, [_P, _I64, _I64, _P]),
+    "fs_expand_tiles": (ctypes.c_int, [_P, _I64, _I64, _P, _P]),
     "fs_ozaki_geometry": (ctypes.c_int, [_P, _P, _P, _P]),
     "fs_ozaki_split": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P]),
     "fs_ozaki_gemm": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I32, _P, _P]),
@@ -330,7 +333,7 @@ CALL_COUNTS = {}
 # kernels each entry point launches
 LAUNCHES_PER_CALL = {
     "fs_abelian_permute": 1, "fs_abelian_permute_multi": 1, "fs_su2_permute_fused": 1, "fs_grouped_dgemm": 1, "fs_grouped_dgemm_thin": 1,
-    "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_ozaki_split": 2,
+    "fs_grouped_dgemm_uniform": 1, "fs_splitk_reduce": 1, "fs_expand_tiles": 1, "fs_ozaki_split": 2,
     "fs_ozaki_gemm": 1, "fs_ozaki_gemm_pair": 1, "fs_ozaki2_split": 2, "fs_ozaki2_gemm_pair": 1,
     "fs_scale": 1, "fs_scale_by": 1, "fs_axpby": 1, "fs_pow": 1, "fs_weighted_sumsq": 2,
     "fs_weighted_sum": 2, "fs_pair_contract": 2, "fs_diag_mul": 1, "fs_o2_recombine": 1,

@@ -11,7 +11,8 @@ recorded set of launches (classes = the bit lengths of M, N and K), a launch of
 copies of the class's largest problem on each path with random operands, and
 keeps the seconds per FLOP; grouped_gemm then sends each problem to the path
 with the smaller predicted time.  Problems of classes that were never measured
-fall back to the analytic cost model.
+take the choice of the nearest measured classes (bit lengths within 2), else the
+analytic cost model.
 
 Typical use: record the launches of one untimed iteration
 (linalg.record_gemm_calls), then tune(records, mode) before timing.
@@ -133,11 +134,38 @@ def tune(records, mode, *, reps=2, min_flops=1e8):
     return n, time.perf_counter() - t0
 
 
-def decide(arr, mode):
-    """Per problem of `arr`: True (mixed path), False (FP64) or None (class not
-    measured)."""
+def _choice(mode, key, max_dist):
+    """True / False from the measured row of `key`, else from the measured
+    classes nearest to it (L1 distance of the bit lengths, at most max_dist;
+    FP64 when the nearest ones disagree), else None."""
+    row = _TABLE.get((mode, key))
+    if row is not None:
+        return bool(row["mixed"] < row["fp64"])
+    best, votes = None, set()
+    for (m, k), r in _TABLE.items():
+        if m != mode:
+            continue
+        d = sum(abs(a - b) for a, b in zip(k, key, strict=True))
+        if d > max_dist or (best is not None and d > best):
+            continue
+        if best is None or d < best:
+            best, votes = d, set()
+        votes.add(bool(r["mixed"] < r["fp64"]))
+    if best is None:
+        return None
+    return votes == {True}
+
+
+def decide(arr, mode, *, max_dist=2):
+    """Per problem of `arr`: True (mixed path), False (FP64) or None (no
+    measured class within max_dist).  A class that was not measured (block
+    sizes drift across a power of two between iterations) takes the decision of
+    its nearest measured neighbours."""
     out = []
+    memo = {}
     for i in range(arr.size):
-        row = _TABLE.get((mode, shape_class(arr["M"][i], arr["N"][i], arr["K"][i])))
-        out.append(None if row is None else bool(row["mixed"] < row["fp64"]))
+        key = shape_class(arr["M"][i], arr["N"][i], arr["K"][i])
+        if key not in memo:
+            memo[key] = _choice(mode, key, max_dist)
+        out.append(memo[key])
     return out

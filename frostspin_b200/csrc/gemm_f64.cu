@@ -520,3 +520,42 @@ extern "C" int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items,
                            fsb::as_stream(stream)>>>(d_items, n_items);
     return fsb::launch_status();
 }
+
+// Tile table from runs (see FsTileRun): one thread per tile, binary search of
+// its run over the sorted run starts.
+namespace fsb {
+
+__global__ void __launch_bounds__(256)
+    k_expand_tiles(const FsTileRun* __restrict__ runs, int64_t n_runs, int64_t total,
+                   FsGemmTile* __restrict__ tiles) {
+    for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        int64_t lo = 0, hi = n_runs - 1;   // last run with start <= t
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (__ldg(&runs[mid].start) <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const FsTileRun r = runs[lo];
+        const int64_t k = t - r.start;
+        const int32_t nc = r.ncol > 0 ? r.ncol : 1;
+        tiles[t] = FsGemmTile{r.problem, static_cast<int32_t>(k / nc),
+                              static_cast<int32_t>(k % nc), 0};
+    }
+}
+
+}  // namespace fsb
+
+extern "C" int fs_expand_tiles(const FsTileRun* d_runs, int64_t n_runs, int64_t total,
+                               FsGemmTile* d_tiles, void* stream) {
+    if (n_runs < 0 || total < 0) return FS_ERR_INVALID_ARG;
+    if (total == 0) return FS_OK;
+    if (n_runs == 0 || d_runs == nullptr || d_tiles == nullptr) return FS_ERR_INVALID_ARG;
+    const int64_t blocks = (total + 255) / 256;
+    const int grid = static_cast<int>(blocks < 8 * fsb::num_sms() ? blocks : 8 * fsb::num_sms());
+    fsb::k_expand_tiles<<<grid, 256, 0, fsb::as_stream(stream)>>>(d_runs, n_runs, total,
+                                                                  d_tiles);
+    return fsb::launch_status();
+}

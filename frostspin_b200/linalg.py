@@ -269,13 +269,9 @@ def grouped_dgemm_table(arr, region="gemm_fp64"):
     if thin.any():
         sub = arr[thin]
         nt = (N[thin] + thin_n - 1) // thin_n
-        total = int(nt.sum())
-        tiles = np.zeros(total, dtype=_native.GEMM_TILE_DTYPE)
-        pid = np.repeat(np.arange(sub.size), nt)
-        tiles["problem"] = pid
-        tiles["tn"] = np.arange(total) - np.repeat(np.cumsum(nt) - nt, nt)
+        runs, total = _tile_runs(nt, nt, np.arange(sub.size))
         d_prob = dev.upload(sub)
-        d_tiles = dev.upload(tiles)
+        d_tiles = _device_tiles(runs, total)
         flops = 2.0 * float((M[thin].astype(np.float64) * N[thin] * K[thin]).sum())
         with instrument.region(region + "_thin", flops=flops,
                                bytes=8.0 * float((N[thin] * (M[thin] + K[thin])).sum())):
@@ -353,19 +349,37 @@ def ozaki2_pays(arr, nmod):
     return t_oz < t_64
 
 
+def _tile_runs(ntile, ncol, order):
+    """FsTileRun table: the problems in `order`, each a run of ntile tiles over
+    ncol tile columns."""
+    nt = np.asarray(ntile, dtype=np.int64)[order]
+    runs = np.zeros(order.size, dtype=_native.TILE_RUN_DTYPE)
+    runs["start"] = np.cumsum(nt) - nt
+    runs["problem"] = order
+    runs["ncol"] = np.asarray(ncol, dtype=np.int64)[order]
+    return runs, int(nt.sum())
+
+
+def _device_tiles(runs, total):
+    """The tile table of a launch, expanded on the device (fs_expand_tiles):
+    only the per-problem runs cross PCIe, not one entry per output tile."""
+    d_tiles = torch.empty(max(total, 1) * _native.GEMM_TILE_DTYPE.itemsize, dtype=torch.uint8,
+                          device=dev.device())
+    keep = runs[runs["start"] < total] if total else runs[:0]
+    if total:
+        d_runs = dev.upload(keep)
+        _native.call("fs_expand_tiles", d_runs.data_ptr(), keep.size, total,
+                     d_tiles.data_ptr(), dev.stream())
+    return d_tiles
+
+
 def _tile_table(arr, tm, tn, ntile):
-    total = int(ntile.sum())
-    tiles = np.zeros(total, dtype=_native.GEMM_TILE_DTYPE)
-    pid = np.repeat(np.arange(arr.size), ntile)
-    first = np.repeat(np.cumsum(ntile) - ntile, ntile)
-    k = np.arange(total) - first
+    """Device tile table of a DMMA launch: largest K first (long tiles start
+    early in the static schedule), each problem's tiles row-major."""
+    order = np.argsort(-arr["K"].astype(np.int64), kind="stable")
     ncol = (arr["N"].astype(np.int64) + tn - 1) // tn
-    tiles["problem"] = pid
-    tiles["tm"] = k // ncol[pid]
-    tiles["tn"] = k % ncol[pid]
-    # largest problems first: long tiles start early in the static schedule
-    order = np.argsort(-arr["K"][pid].astype(np.int64), kind="stable")
-    return tiles[order]
+    runs, total = _tile_runs(ntile, ncol, order)
+    return _device_tiles(runs, total), total
 
 
 _SPLITK_CHUNK = 1024        # smallest K chunk of a split problem
@@ -443,10 +457,9 @@ def _dgemm(arr, problems, tm, tn, ntile):
     sk = _split_k(arr, tm, tn, ntile)
     if sk is not None:
         arr, ntile, items, work = sk
-        tiles = _tile_table(arr, tm, tn, ntile)
+        d_tiles, n_tiles = _tile_table(arr, tm, tn, ntile)
         d_prob = dev.upload(arr)
-        d_tiles = dev.upload(tiles)
-        _launch_dgemm(arr, d_prob, d_tiles, tiles.size)
+        _launch_dgemm(arr, d_prob, d_tiles, n_tiles)
         d_items = dev.upload(items)
         max_elems = int((items["M"].astype(np.int64) * items["N"]).max())
         for start in range(0, items.size, 65535):
@@ -454,10 +467,9 @@ def _dgemm(arr, problems, tm, tn, ntile):
             _native.call("fs_splitk_reduce", d_items.data_ptr() + start * items.itemsize, cnt,
                          max_elems, dev.stream())
         return d_prob, d_tiles, work
-    tiles = _tile_table(arr, tm, tn, ntile)
+    d_tiles, n_tiles = _tile_table(arr, tm, tn, ntile)
     d_prob = dev.upload(arr)
-    d_tiles = dev.upload(tiles)
-    _launch_dgemm(arr, d_prob, d_tiles, tiles.size)
+    _launch_dgemm(arr, d_prob, d_tiles, n_tiles)
     return d_prob, d_tiles
 
 

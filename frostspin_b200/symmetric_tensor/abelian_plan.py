@@ -133,12 +133,8 @@ def leg_coefficients(signature, nrr):
 def magic_divisor(d):
     """Granlund-Montgomery constants (m, s) for 32-bit division by d >= 1."""
     d = np.asarray(d, dtype=np.uint64)
-    s = np.zeros(d.shape, dtype=np.uint64)
-    while True:
-        grow = (np.uint64(1) << s) < d
-        if not grow.any():
-            break
-        s[grow] += np.uint64(1)
+    # s = ceil(log2 d) = bit length of d - 1 (frexp is exact below 2^53)
+    s = np.frexp((d - np.uint64(1)).astype(np.float64))[1].astype(np.uint64)
     m = ((np.uint64(1) << np.uint64(32)) * ((np.uint64(1) << s) - d)) // d + np.uint64(1)
     return m.astype(np.uint32), s.astype(np.uint32)
 

@@ -255,6 +255,24 @@ typedef struct FsSplitReduce {
 int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items, int64_t max_elems,
                      void* stream);
 
+/*
+ * Tile table of a grouped GEMM launch, written on the device (a planning
+ * helper with no reference counterpart: the reference loops over blocks on the
+ * host).  Run r covers tiles [start_r, start_{r+1}) (the last run ends at
+ * `total`), all of problem `problem`, in row-major order over `ncol` tile
+ * columns: tile start_r + k is (problem, k / ncol, k % ncol).  Runs are sorted
+ * by start, start_0 = 0.  Replaces the host enumeration of every output tile
+ * (millions for the wide sector GEMMs of a chi = 256 CTMRG move).
+ */
+typedef struct FsTileRun {
+    int64_t start;
+    int32_t problem;
+    int32_t ncol;
+} FsTileRun;
+
+int fs_expand_tiles(const FsTileRun* d_runs, int64_t n_runs, int64_t total, FsGemmTile* d_tiles,
+                    void* stream);
+
 /* ------------------------------------- grouped GEMM on tcgen05 (Ozaki int8) */
 /*
  * FP64-class GEMM on the int8 tensor cores (tcgen05.mma kind::i8): every row of

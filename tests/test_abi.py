@@ -47,6 +47,9 @@ def test_invalid_arguments_rejected_without_gpu_work():
     assert lib.fs_scale(None, -1, 1.0, None) == -1
     assert lib.fs_grouped_dgemm(None, 0, None, -5, None) == -1
     assert lib.fs_abelian_permute(None, 0, None, 0, None, 0, None, -1, None, None) == -1
+    assert lib.fs_expand_tiles(None, -1, 4, None, None) == -1
+    assert lib.fs_expand_tiles(None, 0, 4, None, None) == -1
+    assert lib.fs_expand_tiles(None, 0, 0, None, None) == 0
     # zero work is a no-op success
     assert lib.fs_scale(None, 0, 1.0, None) == 0
 
@@ -101,6 +104,7 @@ int main(void) {
   S(FsSplitReduce) F(FsSplitReduce, W) F(FsSplitReduce, C) F(FsSplitReduce, ldc)
   F(FsSplitReduce, slice) F(FsSplitReduce, nslices) F(FsSplitReduce, M)
   F(FsSplitReduce, N) F(FsSplitReduce, alpha) F(FsSplitReduce, beta)
+  S(FsTileRun) F(FsTileRun, start) F(FsTileRun, problem) F(FsTileRun, ncol)
   S(FsO2Term) F(FsO2Term, src_off) F(FsO2Term, rs) F(FsO2Term, cs) F(FsO2Term, ridx_off)
   F(FsO2Term, cidx_off) F(FsO2Term, rcoef_off) F(FsO2Term, ccoef_off)
   S(FsO2Block) F(FsO2Block, out_off) F(FsO2Block, nrows) F(FsO2Block, ncols)
@@ -126,6 +130,7 @@ DTYPES = {
     "FsOz2Operand": _native.OZ2_OPERAND_DTYPE,
     "FsOz2Problem": _native.OZ2_PROBLEM_DTYPE,
     "FsSplitReduce": _native.SPLIT_REDUCE_DTYPE,
+    "FsTileRun": _native.TILE_RUN_DTYPE,
     "FsO2Term": _native.O2_TERM_DTYPE,
     "FsO2Block": _native.O2_BLOCK_DTYPE,
 }

@@ -1,6 +1,6 @@
 """The autotuner's dispatch rule (frostspin_b200/autotune.py) on a hand-made
-table: measured classes follow the measurement, unmeasured ones the cost
-model.  Measuring needs a GPU; the rule does not."""
+table: measured classes follow the measurement, unmeasured ones their nearest
+measured neighbours, and classes with no neighbour the cost model.  Measuring needs a GPU; the rule does not."""
 
 import numpy as np
 
@@ -36,3 +36,26 @@ def test_decide_uses_measured_classes_only():
 def test_shape_classes_are_bit_lengths():
     assert autotune.shape_class(1, 2, 3) == (1, 2, 2)
     assert autotune.shape_class(255, 256, 257) == (8, 9, 9)
+
+
+def test_unmeasured_classes_take_nearest_measured_choice():
+    autotune.clear()
+    mode = "ozaki2_13"
+    big = autotune.shape_class(3000, 3000, 3000)        # (12, 12, 12)
+    thin = autotune.shape_class(100, 5000, 40)          # (7, 13, 6)
+    autotune._TABLE[(mode, big)] = {"fp64": 3e-14, "mixed": 1e-14, "shape": (3000,) * 3}
+    autotune._TABLE[(mode, thin)] = {"fp64": 1e-13, "mixed": 4e-13, "shape": (100, 5000, 40)}
+    try:
+        arr = _arr([(5000, 3000, 3000),     # (13, 12, 12): distance 1 from big
+                    (100, 9000, 40),        # (7, 14, 6): distance 1 from thin
+                    (5000, 5000, 5000),     # (13, 13, 13): distance 3, none near
+                    (7, 7, 7)])
+        assert autotune.decide(arr, mode) == [True, False, None, None]
+        # equidistant neighbours that disagree: FP64
+        mid = autotune.shape_class(3000, 3000, 3000)
+        autotune._TABLE[(mode, (12, 12, 14))] = {"fp64": 1e-14, "mixed": 2e-14,
+                                                  "shape": (3000, 3000, 9000)}
+        assert autotune.decide(_arr([(3000, 3000, 5000)]), mode) == [False]
+        assert mid == (12, 12, 12)
+    finally:
+        autotune.clear()
