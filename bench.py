@@ -122,7 +122,7 @@ class ClockSampler:
         self.file.seek(0)
         rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
         os.unlink(self.file.name)
-        sm, smax, reasons = [], [], set()
+        sm, smax, power, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [x.strip() for x in r]
@@ -133,6 +133,10 @@ class ClockSampler:
                 smax.append(float(r[2]))
             except ValueError:
                 continue
+            try:
+                power.append(float(r[3]))
+            except ValueError:
+                pass
             for name, val in zip(names, r[5:9], strict=True):
                 if val.lower().startswith("active"):
                     reasons.add(name)
@@ -141,6 +145,7 @@ class ClockSampler:
             "sm_max_mhz": float(max(smax)) if smax else None,
             "reasons": sorted(reasons),
             "samples": len(sm),
+            "power_w": float(np.median(power)) if power else None,
         }
 
 
@@ -917,7 +922,10 @@ def run_gemm(args, world, rank, local):
         torch.cuda.synchronize()
         return s.elapsed_time(e) * 1e-3 / args.steps
 
+    clocks = ClockSampler(local)
+    clocks.start()
     t = max_over_ranks(timed(step), world)
+    clk = clocks.stop()
     linalg.check_ozaki_flags()
     err = float((C - A @ B).abs().max() / (A.abs().max() * B.abs().max() * K))
     t_cublas = timed(lambda: torch.matmul(A, B, out=C))
@@ -931,7 +939,33 @@ def run_gemm(args, world, rank, local):
         "config": {"workload": "gemm", "shape": [M, N, K], "precision": args.precision,
                    "cublas_dgemm_tflops": flops / t_cublas / 1e12,
                    "max_err_rel_to_maxA_maxB_n": err},
+        "clocks": clk,
+        "roofline": _gemm_roofline(args.precision, M, N, K, t, clk),
     }
+
+
+def _gemm_roofline(precision, M, N, K, t, clk):
+    """Tensor roofline of one GEMM launch: int8 operations on the padded tile
+    grid (Ozaki forms) or FP64 flops (DMMA) per second against the peak, and
+    the same fraction per SM clock cycle (the kernel runs at the power cap, so
+    the clock it gets is part of the result)."""
+    pad = lambda x, a: (x + a - 1) // a * a  # noqa: E731
+    hbm, bf16, kind = load_peaks()
+    if precision.startswith("ozaki2_"):
+        ops = 2.0 * pad(M, 256) * pad(N, 256) * pad(K, 128) * int(precision[7:])
+        peak, unit, name = 2.0 * bf16, "TOP/s (int8)", "k_oz_pair<CRT>"
+    elif precision.startswith("ozaki"):
+        S = int(precision[5:])
+        ops = 2.0 * pad(M, 128) * pad(N, 256) * pad(K, 128) * S * (S + 1) / 2
+        peak, unit, name = 2.0 * bf16, "TOP/s (int8)", "k_oz_gemm_pair"
+    else:
+        return None
+    ach = ops / t / 1e12
+    out = {"bound": "tensor", "kernel": name, "achieved": ach, "peak": peak, "unit": unit,
+           "frac": ach / peak, "peak_kind": f"2 x {kind} bf16 dense", "traffic": None}
+    if clk.get("sm_mhz") and clk.get("sm_max_mhz"):
+        out["frac_per_clock"] = ach / peak * clk["sm_max_mhz"] / clk["sm_mhz"]
+    return out
 
 
 def run_reference_ctmrg(args, world):
