@@ -13,11 +13,15 @@ symmetry, D = 24 (whole multiplets: Dmax = 28), chi = 256.  `--symmetry u1`
 runs the same chain with U(1) sectors (defaults D = 12, chi = 64).  One step =
 one CTMRG iteration (up, right, down, left moves).  The timed iterations start
 from an environment warmed up for W iterations; the headline arithmetic
-(`--precision`, default ozaki2_13: sector GEMMs on the tcgen05 int8 tensor
-cores, one product per modulus for 13 moduli, CRT in FP64; the autotuner picks
-the int8 or FP64 path per sector shape class) runs exactly K iterations, the plain FP64 run (DMMA
-tensor cores) min(K, 3) iterations from a copy of the same environment, and the
-energies per bond after the same number of iterations are compared.
+(`--precision`, default ozaki2_11: sector GEMMs on the tcgen05 int8 tensor
+cores, one product per modulus for 11 moduli, CRT in FP64; the autotuner picks
+the int8 or FP64 path per sector shape class) runs exactly K iterations after
+one untimed iteration of its own, the plain FP64 run (DMMA tensor cores)
+min(K, 3) iterations from a copy of the same environment, and the energies per
+bond after the same number of iterations are compared.  11 moduli are the
+fewest that keep every mixed parity test against the reference's runs within
+its tolerance (10 moduli miss the simple-update logZ bound) and the energy
+within 1e-12 of plain FP64 over 25 iterations.
 
 Workload "u1_microbench": the U(1) kernel microbenchmark -- rank-4 float64
 tensors whose legs carry charges -4..4 with degeneracies ~ exp(-q^2/8) rounded
@@ -390,7 +394,7 @@ def run_ctmrg(args, world, rank, local):
 
     from frostspin_b200 import linalg
 
-    mixed = args.precision if args.precision != "fp64" else "ozaki2_13"
+    mixed = args.precision if args.precision != "fp64" else "ozaki2_11"
     su, tensors, ctm, t_su = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
     # the warm-up iterations record the sector GEMM launches; the tuner
@@ -416,6 +420,17 @@ def run_ctmrg(args, world, rank, local):
                      "classes_total": sum(1 for (m, _) in autotune.table() if m == mixed)}
     start_env = ctm.copy()
     headline_mixed = args.precision != "fp64"
+    if headline_mixed:
+        # one untimed mixed iteration on a throwaway copy: the warm-up above
+        # ran the FP64 path only, and the first int8 iteration pays one-time
+        # costs (slice workspaces and residue scratch growing the allocator's
+        # segments, plans of the new launch shapes)
+        warm = start_env.copy()
+        linalg.set_gemm_precision(mixed)
+        warm.iterate()
+        del warm
+        linalg.set_gemm_precision("fp64")
+        torch.cuda.synchronize()
     # the headline run times exactly `steps` iterations; the comparison run
     # (the other arithmetic, same start environment) is capped at 3 iterations
     # and both energies are taken after the same number of iterations
@@ -429,15 +444,15 @@ def run_ctmrg(args, world, rank, local):
     t64, clk64, k64, l64 = timed_iterations(ctm, n64, "fp64", local)
     chi_values = [int(c) for c in ctm.chi_values]
     e64 = energy_per_bond(ctm) if n64 == n_cmp else None
+    # freed, not released: the mixed run reuses the mapped segments (releasing
+    # them made its first iteration map tens of GB again)
     del ctm
-    torch.cuda.empty_cache()
     ctm_mixed = start_env.copy()
     barrier(world)
     tmx, clkmx, kmx, lmx = timed_iterations(ctm_mixed, nmx, mixed, local)
     emx = energy_per_bond(ctm_mixed) if nmx == n_cmp else None
     if args.symmetry != "u1":
         del ctm_mixed
-    torch.cuda.empty_cache()
     for prec in ("fp64", mixed):
         if (e64 if prec == "fp64" else emx) is not None:
             continue
@@ -450,7 +465,6 @@ def run_ctmrg(args, world, rank, local):
         else:
             emx = energy_per_bond(env)
         del env
-        torch.cuda.empty_cache()
     t64 = max_over_ranks(t64, world)
     tmx = max_over_ranks(tmx, world)
     t_head = tmx if headline_mixed else t64
@@ -476,7 +490,6 @@ def run_ctmrg(args, world, rank, local):
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(es.elapsed_time(ee) * 1e-3, world)
     del e2e_env, new
-    torch.cuda.empty_cache()
     h2d = int(sum(h.numel() * 8 for h in hostA))
     d2h = int(4 * 2 * 16 * 8)  # four 2x2x2x2 reduced density matrices per site pair
 
@@ -1115,7 +1128,7 @@ def run_deviation(args, world, rank, local):
 
     from frostspin_b200 import autotune, linalg
 
-    mixed = args.precision if args.precision != "fp64" else "ozaki2_13"
+    mixed = args.precision if args.precision != "fp64" else "ozaki2_11"
     points = sorted(int(x) for x in args.deviation.split(","))
     su, tensors, ctm, _ = ctmrg_setup(args)
     linalg.set_gemm_precision("fp64")
@@ -1419,7 +1432,7 @@ def main():
                     help="chi values the CPU reference arm of the ctmrg workload measures")
     ap.add_argument("--ozaki-pair", choices=["on", "off"], default="on",
                     help="large int8 sector GEMMs on CTA pairs (tcgen05 cta_group::2)")
-    ap.add_argument("--precision", default="ozaki2_13",
+    ap.add_argument("--precision", default="ozaki2_11",
                     help="sector GEMM arithmetic: fp64, ozakiS (S = 3..8 int8 digit slices) "
                          "or ozaki2_N (N = 8..14 int8 moduli, CRT)")
     ap.add_argument("--leg-states", type=int, default=LEG_STATES,

@@ -388,48 +388,70 @@ namespace fsb {
 
 constexpr int kThinMax = 32;
 constexpr int kThinThreads = 128;
-constexpr int kThinColsPerThread = 2;
+constexpr int kThinColsPerThread = 4;
 
-template <int MB>
+// MB, KB: M and K rounded up to 4, 8, 16 or 32; NC: columns a thread carries
+// at once (KB * NC <= 32 doubles of operands in registers).  Every load of a
+// pass (KB per column, predicated on k < K) is issued before its FMAs, so each
+// thread keeps up to 32 loads in flight: with the k loop rolled, one load per
+// column at a time left the kernel latency bound at a third of the HBM
+// bandwidth.
+template <int MB, int KB, int NC>
 __device__ __forceinline__ void thin_tile(const FsGemmProblem& p, const double* su, int n0) {
-    double acc[kThinColsPerThread][MB];
 #pragma unroll
-    for (int c = 0; c < kThinColsPerThread; ++c)
+    for (int c0 = 0; c0 < kThinColsPerThread; c0 += NC) {
+        int cols[NC];
+        bool ok[NC];
 #pragma unroll
-        for (int m = 0; m < MB; ++m) acc[c][m] = 0.0;
-    int cols[kThinColsPerThread];
-    bool ok[kThinColsPerThread];
+        for (int c = 0; c < NC; ++c) {
+            cols[c] = n0 + threadIdx.x + (c0 + c) * kThinThreads;
+            ok[c] = cols[c] < p.N;
+        }
+        double x[KB][NC];
 #pragma unroll
-    for (int c = 0; c < kThinColsPerThread; ++c) {
-        cols[c] = n0 + threadIdx.x + c * kThinThreads;
-        ok[c] = cols[c] < p.N;
-    }
-    for (int k = 0; k < p.K; ++k) {
-        double x[kThinColsPerThread];
+        for (int k = 0; k < KB; ++k)
 #pragma unroll
-        for (int c = 0; c < kThinColsPerThread; ++c)
-            x[c] = ok[c] ? __ldg(p.B + static_cast<int64_t>(k) * p.ldb + cols[c]) : 0.0;
+            for (int c = 0; c < NC; ++c)
+                x[k][c] = (ok[c] && k < p.K)
+                              ? __ldg(p.B + static_cast<int64_t>(k) * p.ldb + cols[c])
+                              : 0.0;
 #pragma unroll
         for (int m = 0; m < MB; ++m) {
-            const double u = su[m * kThinMax + k];
+            if (m >= p.M) break;
+            double acc[NC];
 #pragma unroll
-            for (int c = 0; c < kThinColsPerThread; ++c) acc[c][m] = fma(u, x[c], acc[c][m]);
-        }
-    }
+            for (int c = 0; c < NC; ++c) acc[c] = 0.0;
 #pragma unroll
-    for (int m = 0; m < MB; ++m) {
-        if (m >= p.M) break;
+            for (int k = 0; k < KB; ++k) {
+                // su holds zeros for k >= K (the staging pads the rows)
+                const double u = su[m * kThinMax + k];
 #pragma unroll
-        for (int c = 0; c < kThinColsPerThread; ++c) {
-            if (!ok[c]) continue;
-            double* dst = p.C + static_cast<int64_t>(m) * p.ldc + cols[c];
-            const double v = p.alpha * acc[c][m];
-            *dst = (p.beta == 0.0) ? v : fma(p.beta, *dst, v);
+                for (int c = 0; c < NC; ++c) acc[c] = fma(u, x[k][c], acc[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (!ok[c]) continue;
+                double* dst = p.C + static_cast<int64_t>(m) * p.ldc + cols[c];
+                const double v = p.alpha * acc[c];
+                *dst = (p.beta == 0.0) ? v : fma(p.beta, *dst, v);
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(kThinThreads)
+template <int MB>
+__device__ __forceinline__ void thin_tile_k(const FsGemmProblem& p, const double* su, int n0) {
+    if (p.K <= 4)
+        thin_tile<MB, 4, 4>(p, su, n0);
+    else if (p.K <= 8)
+        thin_tile<MB, 8, 4>(p, su, n0);
+    else if (p.K <= 16)
+        thin_tile<MB, 16, 2>(p, su, n0);
+    else
+        thin_tile<MB, 32, 1>(p, su, n0);
+}
+
+__global__ void __launch_bounds__(kThinThreads, 4)
     k_grouped_dgemm_thin(const FsGemmProblem* __restrict__ problems, int64_t n_problems,
                          const FsGemmTile* __restrict__ tiles, int64_t n_tiles) {
     __shared__ double su[kThinMax * kThinMax];
@@ -442,22 +464,22 @@ __global__ void __launch_bounds__(kThinThreads)
         const int n0 = tile.tn * kCols;
         if (n0 >= p.N) continue;
         __syncthreads();  // previous tile's reads of su are done
-        // only the M x K entries are staged (rows beyond M are never read, and
-        // the k loop stops at K)
-        const int mk = p.M * p.K;
+        // rows m < M of U, zero-padded to kThinMax columns (the unrolled k
+        // loop reads up to K rounded up)
+        const int mk = p.M * kThinMax;
         for (int i = threadIdx.x; i < mk; i += kThinThreads) {
-            const int m = i / p.K, k = i - m * p.K;
-            su[m * kThinMax + k] = p.A[static_cast<int64_t>(m) * p.lda + k];
+            const int m = i / kThinMax, k = i - m * kThinMax;
+            su[i] = (k < p.K) ? p.A[static_cast<int64_t>(m) * p.lda + k] : 0.0;
         }
         __syncthreads();
         if (p.M <= 4)
-            thin_tile<4>(p, su, n0);
+            thin_tile_k<4>(p, su, n0);
         else if (p.M <= 8)
-            thin_tile<8>(p, su, n0);
+            thin_tile_k<8>(p, su, n0);
         else if (p.M <= 16)
-            thin_tile<16>(p, su, n0);
+            thin_tile_k<16>(p, su, n0);
         else
-            thin_tile<32>(p, su, n0);
+            thin_tile_k<32>(p, su, n0);
     }
 }
 

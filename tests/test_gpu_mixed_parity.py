@@ -19,7 +19,9 @@ pytestmark = pytest.mark.gpu
 SDS = np.array([[0.25, 0, 0, 0], [0, -0.25, 0.5, 0], [0, 0.5, -0.25, 0],
                 [0, 0, 0, 0.25]]).reshape(2, 2, 2, 2)
 
-MIXED = ["ozaki7", "ozaki2_13", "ozaki2_14"]
+# ozaki2_11 is the benchmark's default, the fewest moduli that pass both
+# tests (10 moduli give a simple-update logZ 3e-11 from the reference's)
+MIXED = ["ozaki7", "ozaki2_11", "ozaki2_12", "ozaki2_13", "ozaki2_14"]
 
 
 @pytest.mark.parametrize("precision", MIXED)
