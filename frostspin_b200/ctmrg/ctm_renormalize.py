@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from .. import linalg
-from ..misc_tools.svd_tools import find_block_cuts, truncated_svd_block
+from ..misc_tools.svd_tools import find_block_cuts, truncated_svd_blocks
 
 
 def _block_index(tensor, irreps):
@@ -61,13 +61,11 @@ def construct_projectors(
     _, _, _, m_blocks = linalg.matmul_blocks(r_blocks, rt_blocks)
 
     dims = np.array([corner2.irrep_dimension(corner2.block_irreps[i]) for i in i2], dtype=int)
-    u_blocks, s_blocks, v_blocks = [], [], []
+    fulls = []
     for bi, m in enumerate(m_blocks):
         ncv = int(ncv_ratio * block_chi[bi]) + 10
-        u, s, v = truncated_svd_block(m, int(block_chi[bi]), full=min(m.shape) < max(100, 4 * ncv))
-        u_blocks.append(u)
-        s_blocks.append(s)
-        v_blocks.append(v)
+        fulls.append(min(m.shape) < max(100, 4 * ncv))
+    u_blocks, s_blocks, v_blocks = truncated_svd_blocks(m_blocks, block_chi, fulls)
 
     host_s = [s.detach().cpu().numpy() for s in s_blocks]
     cuts = find_block_cuts(host_s, chi_target, dims=dims, atol=atol, rtol=rtol,

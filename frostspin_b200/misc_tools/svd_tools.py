@@ -51,6 +51,72 @@ def truncated_svd_block(m, k, *, full, n_iter=3, oversampling=None):
     return u[:, :k], s[:k], vh[:k]
 
 
+def truncated_svd_blocks(blocks, ks, fulls, *, n_iter=3, oversampling=None):
+    """truncated_svd_block for many device blocks at once, with the same
+    arithmetic per block (same seeds, same steps): the randomized blocks
+    advance in lock step, every product of a step in one grouped GEMM launch
+    over all of them, and the SVDs that synchronise with the host (cuSOLVER
+    checks its status) come last, so that the device never waits for the host
+    to plan the next block.  Returns lists (U, s, Vh)."""
+    from .. import instrument, linalg
+
+    n = len(blocks)
+    out_u, out_s, out_v = [None] * n, [None] * n, [None] * n
+    dense, rand = [], []
+    for i, m in enumerate(blocks):
+        nr, nc = m.shape
+        if fulls[i] or ks[i] >= min(nr, nc) // 2:
+            dense.append(i)
+        else:
+            rand.append(i)
+    if rand:
+        ms = [blocks[i] for i in rand]
+        omegas = []
+        for i in rand:
+            m = blocks[i]
+            nr, nc = m.shape
+            k = int(ks[i])
+            p = k + 10 if oversampling is None else oversampling
+            kk = min(min(nr, nc), k + p)
+            g = torch.Generator(device=m.device)
+            g.manual_seed(1234 + nr * 7 + nc)
+            omegas.append(torch.randn(nc, kk, dtype=m.dtype, device=m.device, generator=g))
+
+        def qr_all(ys):
+            out = []
+            for y in ys:
+                with instrument.region("svd_qr"):
+                    q, _ = torch.linalg.qr(y, mode="reduced")
+                out.append(q)
+            return out
+
+        _, _, _, ys = linalg.matmul_blocks(ms, omegas)
+        qs = qr_all(ys)
+        for _ in range(n_iter):
+            _, _, _, zs = linalg.matmul_blocks([m.T for m in ms], qs)
+            zs = qr_all(zs)
+            _, _, _, ys = linalg.matmul_blocks(ms, zs)
+            qs = qr_all(ys)
+        _, _, _, bs = linalg.matmul_blocks([q.T for q in qs], ms)
+        ubs = []
+        for j, i in enumerate(rand):
+            with instrument.region("svd_small"):
+                ub, sv, vh = torch.linalg.svd(bs[j], full_matrices=False)
+            k = int(ks[i])
+            ubs.append(ub)
+            out_s[i] = sv[:k]
+            out_v[i] = vh[:k]
+        _, _, _, us = linalg.matmul_blocks(qs, ubs)
+        for j, i in enumerate(rand):
+            out_u[i] = us[j][:, : int(ks[i])]
+    for i in dense:
+        m = blocks[i]
+        with instrument.region("svd_dense", elems=float(m.shape[0] * m.shape[1])):
+            u, sv, vh = torch.linalg.svd(m, full_matrices=False)
+        out_u[i], out_s[i], out_v[i] = u, sv, vh
+    return out_u, out_s, out_v
+
+
 def find_block_cuts(block_values, cut_target, *, dims=None, atol=0.0, rtol=None,
                     degen_ratio=1.0):
     """Number of values to keep per block.
