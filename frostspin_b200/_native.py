@@ -98,7 +98,8 @@ GEMM_TILE_DTYPE = np.dtype(
     [("problem", "<i4"), ("tm", "<i4"), ("tn", "<i4"), ("pad", "<i4")]
 )
 
-TILE_RUN_DTYPE = np.dtype([("start", "<i8"), ("problem", "<i4"), ("ncol", "<i4")])
+TILE_RUN_DTYPE = np.dtype([("start", "<i8"), ("problem", "<i4"), ("ncol", "<i4"),
+                           ("nrow", "<i4"), ("col_major", "<i4")])
 
 SPLIT_REDUCE_DTYPE = np.dtype(
     [

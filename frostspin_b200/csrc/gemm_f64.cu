@@ -562,9 +562,15 @@ __global__ void __launch_bounds__(256)
         }
         const FsTileRun r = runs[lo];
         const int64_t k = t - r.start;
-        const int32_t nc = r.ncol > 0 ? r.ncol : 1;
-        tiles[t] = FsGemmTile{r.problem, static_cast<int32_t>(k / nc),
-                              static_cast<int32_t>(k % nc), 0};
+        if (r.col_major) {
+            const int32_t nr = r.nrow > 0 ? r.nrow : 1;
+            tiles[t] = FsGemmTile{r.problem, static_cast<int32_t>(k % nr),
+                                  static_cast<int32_t>(k / nr), 0};
+        } else {
+            const int32_t nc = r.ncol > 0 ? r.ncol : 1;
+            tiles[t] = FsGemmTile{r.problem, static_cast<int32_t>(k / nc),
+                                  static_cast<int32_t>(k % nc), 0};
+        }
     }
 }
 

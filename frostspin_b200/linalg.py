@@ -349,14 +349,22 @@ def ozaki2_pays(arr, nmod):
     return t_oz < t_64
 
 
-def _tile_runs(ntile, ncol, order):
+def _tile_runs(ntile, ncol, order, nrow=None):
     """FsTileRun table: the problems in `order`, each a run of ntile tiles over
-    ncol tile columns."""
+    nrow x ncol tiles; problems with more tile columns than rows run
+    column-major (their few row tiles share each B column block in L2)."""
     nt = np.asarray(ntile, dtype=np.int64)[order]
     runs = np.zeros(order.size, dtype=_native.TILE_RUN_DTYPE)
     runs["start"] = np.cumsum(nt) - nt
     runs["problem"] = order
-    runs["ncol"] = np.asarray(ncol, dtype=np.int64)[order]
+    nc = np.asarray(ncol, dtype=np.int64)[order]
+    runs["ncol"] = nc
+    if nrow is not None:
+        nr = np.asarray(nrow, dtype=np.int64)[order]
+        runs["nrow"] = nr
+        runs["col_major"] = nc > nr
+    else:
+        runs["nrow"] = 1
     return runs, int(nt.sum())
 
 
@@ -378,7 +386,8 @@ def _tile_table(arr, tm, tn, ntile):
     early in the static schedule), each problem's tiles row-major."""
     order = np.argsort(-arr["K"].astype(np.int64), kind="stable")
     ncol = (arr["N"].astype(np.int64) + tn - 1) // tn
-    runs, total = _tile_runs(ntile, ncol, order)
+    nrow = (arr["M"].astype(np.int64) + tm - 1) // tm
+    runs, total = _tile_runs(ntile, ncol, order, nrow)
     return _device_tiles(runs, total), total
 
 

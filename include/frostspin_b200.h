@@ -259,8 +259,10 @@ int fs_splitk_reduce(const FsSplitReduce* d_items, int64_t n_items, int64_t max_
  * Tile table of a grouped GEMM launch, written on the device (a planning
  * helper with no reference counterpart: the reference loops over blocks on the
  * host).  Run r covers tiles [start_r, start_{r+1}) (the last run ends at
- * `total`), all of problem `problem`, in row-major order over `ncol` tile
- * columns: tile start_r + k is (problem, k / ncol, k % ncol).  Runs are sorted
+ * `total`), all of problem `problem`, over nrow x ncol tiles: tile start_r + k
+ * is (problem, k / ncol, k % ncol) in row-major order, or (problem, k % nrow,
+ * k / nrow) when col_major is set (wide problems: the few row tiles of a
+ * column block run side by side and share its B tile in L2).  Runs are sorted
  * by start, start_0 = 0.  Replaces the host enumeration of every output tile
  * (millions for the wide sector GEMMs of a chi = 256 CTMRG move).
  */
@@ -268,6 +270,8 @@ typedef struct FsTileRun {
     int64_t start;
     int32_t problem;
     int32_t ncol;
+    int32_t nrow;
+    int32_t col_major;
 } FsTileRun;
 
 int fs_expand_tiles(const FsTileRun* d_runs, int64_t n_runs, int64_t total, FsGemmTile* d_tiles,

@@ -105,6 +105,7 @@ int main(void) {
   F(FsSplitReduce, slice) F(FsSplitReduce, nslices) F(FsSplitReduce, M)
   F(FsSplitReduce, N) F(FsSplitReduce, alpha) F(FsSplitReduce, beta)
   S(FsTileRun) F(FsTileRun, start) F(FsTileRun, problem) F(FsTileRun, ncol)
+  F(FsTileRun, nrow) F(FsTileRun, col_major)
   S(FsO2Term) F(FsO2Term, src_off) F(FsO2Term, rs) F(FsO2Term, cs) F(FsO2Term, ridx_off)
   F(FsO2Term, cidx_off) F(FsO2Term, rcoef_off) F(FsO2Term, ccoef_off)
   S(FsO2Block) F(FsO2Block, out_off) F(FsO2Block, nrows) F(FsO2Block, ncols)

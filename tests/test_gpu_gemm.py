@@ -165,21 +165,24 @@ def test_split_k_for_launches_with_few_tiles(trans_a, trans_b):
 
 
 def test_device_tile_table_matches_host_enumeration():
-    """fs_expand_tiles writes the tile list the host used to enumerate: every
-    problem's tiles row-major, problems in the given order, empty problems
-    skipped."""
+    """fs_expand_tiles writes the tile list: every problem's tiles row-major,
+    or column-major for wide problems, problems in the given order, empty
+    problems skipped."""
     import torch
 
     from frostspin_b200 import _native, linalg
 
-    ntile = np.array([6, 0, 1, 12, 0, 5, 0], dtype=np.int64)
-    ncol = np.array([3, 4, 1, 4, 2, 5, 1], dtype=np.int64)
+    ncol = np.array([3, 4, 1, 2, 2, 5, 1], dtype=np.int64)
+    nrow = np.array([2, 0, 1, 6, 0, 1, 0], dtype=np.int64)
+    ntile = ncol * nrow
     order = np.array([3, 1, 0, 6, 2, 5, 4])
-    runs, total = linalg._tile_runs(ntile, ncol, order)
+    runs, total = linalg._tile_runs(ntile, ncol, order, nrow)
     d_tiles = linalg._device_tiles(runs, total)
     torch.cuda.synchronize()
     got = d_tiles.cpu().numpy()[: total * _native.GEMM_TILE_DTYPE.itemsize].view(
         _native.GEMM_TILE_DTYPE)
-    want = [(p, k // ncol[p], k % ncol[p]) for p in order for k in range(ntile[p])]
+    # wide problems (more tile columns than rows) column-major, the rest row-major
+    want = [(p, k % nrow[p], k // nrow[p]) if ncol[p] > nrow[p] else (p, k // ncol[p], k % ncol[p])
+            for p in order for k in range(ntile[p])]
     assert total == len(want)
     assert [tuple(int(x) for x in (t["problem"], t["tm"], t["tn"])) for t in got] == want
