@@ -51,6 +51,19 @@ def truncated_svd_block(m, k, *, full, n_iter=3, oversampling=None):
     return u[:, :k], s[:k], vh[:k]
 
 
+_QR_STREAMS = 4
+_STREAMS = {}
+
+
+def _qr_streams():
+    dev = torch.cuda.current_device()
+    st = _STREAMS.get(dev)
+    if st is None:
+        st = [torch.cuda.Stream(device=dev) for _ in range(_QR_STREAMS)]
+        _STREAMS[dev] = st
+    return st
+
+
 def truncated_svd_blocks(blocks, ks, fulls, *, n_iter=3, oversampling=None):
     """truncated_svd_block for many device blocks at once, with the same
     arithmetic per block (same seeds, same steps): the randomized blocks
@@ -83,11 +96,26 @@ def truncated_svd_blocks(blocks, ks, fulls, *, n_iter=3, oversampling=None):
             omegas.append(torch.randn(nc, kk, dtype=m.dtype, device=m.device, generator=g))
 
         def qr_all(ys):
+            # the QRs of the blocks are independent and each is a chain of
+            # small panel kernels: spread them over side streams so that they
+            # overlap, then join the main stream before the next grouped GEMM
+            main = torch.cuda.current_stream()
+            ready = torch.cuda.Event()
+            ready.record(main)
             out = []
-            for y in ys:
-                with instrument.region("svd_qr"):
-                    q, _ = torch.linalg.qr(y, mode="reduced")
-                out.append(q)
+            with instrument.region("svd_qr"):
+                for j, y in enumerate(ys):
+                    side = _qr_streams()[j % _QR_STREAMS]
+                    side.wait_event(ready)
+                    y.record_stream(side)
+                    with torch.cuda.stream(side):
+                        q, _ = torch.linalg.qr(y, mode="reduced")
+                    q.record_stream(main)
+                    out.append(q)
+                for side in _qr_streams()[: min(len(ys), _QR_STREAMS)]:
+                    done = torch.cuda.Event()
+                    done.record(side)
+                    main.wait_event(done)
             return out
 
         _, _, _, ys = linalg.matmul_blocks(ms, omegas)

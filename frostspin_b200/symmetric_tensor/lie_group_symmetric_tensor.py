@@ -41,15 +41,19 @@ from .symmetric_tensor import SymmetricTensor
 
 _MAP_CACHE = OrderedDict()
 _MAP_CACHE_SIZE = 256
-_FUSED = {"on": False, "limits": None}
+_FUSED = {"on": True, "limits": None}
 
 
 def set_fused_permute(enabled):
     """Whether permutes run the simple blocks with small recoupling matrices
-    through the one-pass fused kernel or through gather -> grouped GEMM ->
-    scatter like the others (the default: faster as built, see the kernel's
-    notes); the results agree to rounding."""
+    through the one-pass fused kernel (the default: one pass over the data
+    instead of three) or through gather -> grouped GEMM -> scatter like the
+    others; the results agree to rounding."""
     _FUSED["on"] = bool(enabled)
+
+
+def fused_permute_enabled():
+    return _FUSED["on"]
 
 
 def _fused_limits():

@@ -19,7 +19,8 @@ from .._native import FS_PERM_MAXR, PERM_TASK_DTYPE, SU2_GROUP_DTYPE, SU2_PIECE_
 from .abelian_plan import magic_divisor
 
 MAXD = 8
-TASK_COLUMNS = 1024
+TASK_COLUMNS = 4096
+TASK_ROWS = 48      # FS_SU2_TASK_ROWS: outer-leg values one task may span
 
 
 def fusable(M, K, E, e_out, n_in, n_out, max_rows, max_pieces):
@@ -38,70 +39,71 @@ def build(groups_sel, e_out, E, M, K, u_off, gather, gin_group, gin_row, scatter
     simple block of every piece, gin_row / sout_row its first row in the
     group (structural offset koff / moff).  Input pieces take their strides
     from the source side (ostride, obase; absent sources get base -1), output
-    pieces from the destination side (nstride, nbase)."""
+    pieces from the destination side (nstride, nbase).  Vectorised over the
+    groups: the legs of a group in output order with unit legs dropped, every
+    piece's leg strides reordered the same way."""
     axes = np.asarray(axes, dtype=np.int64)
-    ng = len(groups_sel)
+    sel = np.asarray(groups_sel, dtype=np.int64)
+    ng = sel.size
     gtab = np.zeros(ng, dtype=SU2_GROUP_DTYPE)
     gd, go, _, gob, _, gpres = gather
     sd, _, sn, _, snb, _ = scatter
-    pieces_in, pieces_out = [], []
-    for j, g in enumerate(groups_sel):
-        keep = np.flatnonzero(e_out[g] > 1)
-        dims = e_out[g][keep]
-        pi = np.flatnonzero(gin_group == g)
-        po = np.flatnonzero(sout_group == g)
-        row_in = gin_row[pi]
-        row_out = sout_row[po]
-        tin = np.zeros(pi.size, dtype=SU2_PIECE_DTYPE)
-        tin["base"] = np.where(gpres[pi], gob[pi], -1)
-        tin["sr_stride"] = go[pi, 0]
-        tin["sc_stride"] = go[pi, 1]
-        ext_in = go[pi][:, 2:][:, axes][:, keep]
-        tin["ext"][:, : keep.size] = ext_in
-        tin["sr"] = gd[pi, 0]
-        tin["sc"] = gd[pi, 1]
-        tin["row0"] = row_in
-        tout = np.zeros(po.size, dtype=SU2_PIECE_DTYPE)
-        tout["base"] = snb[po]
-        tout["sr_stride"] = sn[po, 0]
-        tout["sc_stride"] = sn[po, 1]
-        tout["ext"][:, : keep.size] = sn[po][:, 2:][:, keep]
-        tout["sr"] = sd[po, 0]
-        tout["sc"] = sd[po, 1]
-        tout["row0"] = row_out
-        pieces_in.append(tin)
-        pieces_out.append(tout)
-        gtab["u_off"][j] = u_off[g]
-        gtab["ncols"][j] = E[g]
-        gtab["dims"][j] = 1
-        gtab["dims"][j, : keep.size] = dims
-        m, s = magic_divisor(np.maximum(gtab["dims"][j].astype(np.int64), 1))
-        gtab["divm"][j] = m
-        gtab["divs"][j] = s
-        gtab["ndim"][j] = keep.size
-        gtab["M"][j] = M[g]
-        gtab["K"][j] = K[g]
-        gtab["in_count"][j] = pi.size
-        gtab["out_count"][j] = po.size
-    pin = np.concatenate(pieces_in) if pieces_in else np.zeros(0, dtype=SU2_PIECE_DTYPE)
-    pout = np.concatenate(pieces_out) if pieces_out else np.zeros(0, dtype=SU2_PIECE_DTYPE)
-    counts_in = gtab["in_count"].astype(np.int64)
-    counts_out = gtab["out_count"].astype(np.int64)
-    gtab["in_first"] = np.concatenate([[0], np.cumsum(counts_in)[:-1]]) if ng else []
-    gtab["out_first"] = (pin.size + np.concatenate([[0], np.cumsum(counts_out)[:-1]])
-                         if ng else [])
-    pieces = np.concatenate([pin, pout])
-    # tasks: runs of TASK_COLUMNS columns of one group
-    ncols = gtab["ncols"].astype(np.int64)
-    nt = (ncols + TASK_COLUMNS - 1) // TASK_COLUMNS
-    tasks = np.zeros(int(nt.sum()), dtype=PERM_TASK_DTYPE)
-    gi = np.repeat(np.arange(ng), nt)
-    first = np.repeat(np.cumsum(nt) - nt, nt)
-    start = (np.arange(tasks.size) - first) * TASK_COLUMNS
-    tasks["eb"] = gi
-    tasks["start"] = start
-    tasks["count"] = np.minimum(TASK_COLUMNS, ncols[gi] - start)
-    return gtab, pieces, tasks
+    n_sb = e_out.shape[0]
+    nleg = e_out.shape[1]
+    pos = np.full(n_sb, -1, dtype=np.int64)
+    pos[sel] = np.arange(ng)
+    eo = e_out[sel]
+    keep = eo > 1
+    nkeep = keep.sum(axis=1)
+    order = np.argsort(~keep, axis=1, kind="stable")    # kept legs first, in order
+    live = np.arange(nleg)[None, :] < nkeep[:, None]
+    dims = np.where(live, np.take_along_axis(eo, order, axis=1), 1)
+
+    def pieces_of(groups):
+        # the pieces of the selected groups, grouped, in their original order
+        idx = np.flatnonzero(pos[groups] >= 0)
+        return idx[np.argsort(pos[groups[idx]], kind="stable")]
+
+    pi = pieces_of(gin_group)
+    po = pieces_of(sout_group)
+    gi_in = pos[gin_group[pi]]
+    gi_out = pos[sout_group[po]]
+    tin = np.zeros(pi.size, dtype=SU2_PIECE_DTYPE)
+    tin["base"] = np.where(gpres[pi], gob[pi], -1)
+    tin["sr_stride"] = go[pi, 0]
+    tin["sc_stride"] = go[pi, 1]
+    ext_in = np.take_along_axis(go[pi][:, 2:][:, axes], order[gi_in], axis=1)
+    tin["ext"][:, :nleg] = np.where(live[gi_in], ext_in, 0)[:, :MAXD]
+    tin["sr"] = gd[pi, 0]
+    tin["sc"] = gd[pi, 1]
+    tin["row0"] = gin_row[pi]
+    tout = np.zeros(po.size, dtype=SU2_PIECE_DTYPE)
+    tout["base"] = snb[po]
+    tout["sr_stride"] = sn[po, 0]
+    tout["sc_stride"] = sn[po, 1]
+    ext_out = np.take_along_axis(sn[po][:, 2:], order[gi_out], axis=1)
+    tout["ext"][:, :nleg] = np.where(live[gi_out], ext_out, 0)[:, :MAXD]
+    tout["sr"] = sd[po, 0]
+    tout["sc"] = sd[po, 1]
+    tout["row0"] = sout_row[po]
+    gtab["u_off"] = u_off[sel]
+    gtab["ncols"] = E[sel]
+    gtab["dims"] = 1
+    gtab["dims"][:, :nleg] = dims[:, :MAXD]
+    m, sh = magic_divisor(np.maximum(gtab["dims"].astype(np.int64), 1))
+    gtab["divm"] = m
+    gtab["divs"] = sh
+    gtab["ndim"] = nkeep
+    gtab["M"] = M[sel]
+    gtab["K"] = K[sel]
+    counts_in = np.bincount(gi_in, minlength=ng)
+    counts_out = np.bincount(gi_out, minlength=ng)
+    gtab["in_count"] = counts_in
+    gtab["out_count"] = counts_out
+    gtab["in_first"] = np.cumsum(counts_in) - counts_in
+    gtab["out_first"] = pi.size + np.cumsum(counts_out) - counts_out
+    pieces = np.concatenate([tin, tout])
+    return gtab, pieces, make_tasks(gtab)
 
 
 def check(gtab, pieces, src_len, out_len, u_len):
@@ -109,30 +111,62 @@ def check(gtab, pieces, src_len, out_len, u_len):
     before the call; the kernel checks again and flags)."""
     if gtab.size == 0:
         return
-    for j in range(gtab.size):
-        g = gtab[j]
-        nd = int(g["ndim"])
-        if g["u_off"] < 0 or g["u_off"] + int(g["M"]) * int(g["K"]) > u_len:
-            raise AssertionError("recoupling matrix outside the U buffer")
-        for first, count, length, is_in in ((g["in_first"], g["in_count"], src_len, True),
-                                            (g["out_first"], g["out_count"], out_len, False)):
-            rows = 0
-            for p in pieces[int(first): int(first) + int(count)]:
-                rows += int(p["sr"]) * int(p["sc"])
-                if is_in and p["base"] < 0:
-                    continue
-                ext = p["ext"][:nd].astype(np.int64)
-                d = g["dims"][:nd].astype(np.int64) - 1
-                lo = p["base"] + (np.minimum(ext, 0) * d).sum()
-                hi = (p["base"] + (np.maximum(ext, 0) * d).sum()
-                      + (int(p["sr"]) - 1) * int(p["sr_stride"])
-                      + (int(p["sc"]) - 1) * int(p["sc_stride"]))
-                if lo < 0 or hi >= length:
-                    raise AssertionError("fused permute piece outside its buffer")
-                if int(p["row0"]) + int(p["sr"]) * int(p["sc"]) > (g["K"] if is_in else g["M"]):
-                    raise AssertionError("fused permute piece rows outside the group")
-            if rows != (g["K"] if is_in else g["M"]):
-                raise AssertionError("fused permute pieces do not cover the group")
+    if ((gtab["u_off"] < 0) | (gtab["u_off"] + gtab["M"].astype(np.int64) * gtab["K"] > u_len)).any():
+        raise AssertionError("recoupling matrix outside the U buffer")
+    d = gtab["dims"].astype(np.int64) - 1
+    for first, count, length, is_in, rows_key in (
+            ("in_first", "in_count", src_len, True, "K"), ("out_first", "out_count", out_len, False, "M")):
+        cnt = gtab[count].astype(np.int64)
+        idx = np.repeat(gtab[first].astype(np.int64), cnt) + (
+            np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+        gidx = np.repeat(np.arange(gtab.size), cnt)
+        pc = pieces[idx]
+        ext = pc["ext"].astype(np.int64)
+        sr = pc["sr"].astype(np.int64)
+        sc = pc["sc"].astype(np.int64)
+        lo = pc["base"] + (np.minimum(ext, 0) * d[gidx]).sum(axis=1)
+        hi = (pc["base"] + (np.maximum(ext, 0) * d[gidx]).sum(axis=1)
+              + (sr - 1) * pc["sr_stride"] + (sc - 1) * pc["sc_stride"])
+        live = pc["base"] >= 0 if is_in else np.ones(idx.size, dtype=bool)
+        if ((lo < 0) | (hi >= length))[live].any():
+            raise AssertionError("fused permute piece outside its buffer")
+        lim = gtab[rows_key].astype(np.int64)
+        if (pc["row0"] + sr * sc > lim[gidx]).any():
+            raise AssertionError("fused permute piece rows outside the group")
+        if not np.array_equal(np.bincount(gidx, weights=sr * sc, minlength=gtab.size), lim):
+            raise AssertionError("fused permute pieces do not cover the group")
+
+
+def make_tasks(gtab):
+    """Tasks of the fused kernel: whole rows of the innermost output leg (L
+    columns each), at most TASK_ROWS rows and about TASK_COLUMNS columns per
+    task; a row longer than TASK_COLUMNS is cut into pieces of one row."""
+    ng = gtab.size
+    ncols = gtab["ncols"].astype(np.int64)
+    nd = gtab["ndim"].astype(np.int64)
+    L = np.where(nd > 0, gtab["dims"][np.arange(ng), np.maximum(nd - 1, 0)], 1).astype(np.int64)
+    per = np.where(L >= TASK_COLUMNS, TASK_COLUMNS,
+                   L * np.clip(TASK_COLUMNS // np.maximum(L, 1), 1, TASK_ROWS))
+    starts, groups_of = [], []
+    for g in range(ng):
+        if L[g] >= TASK_COLUMNS:
+            rows = np.arange(0, ncols[g], L[g])
+            inner = np.arange(0, L[g], TASK_COLUMNS)
+            st = (rows[:, None] + inner[None, :]).ravel()
+        else:
+            st = np.arange(0, ncols[g], per[g])
+        starts.append(st)
+        groups_of.append(np.full(st.size, g))
+    tasks = np.zeros(int(sum(x.size for x in starts)), dtype=PERM_TASK_DTYPE)
+    if tasks.size == 0:
+        return tasks
+    st = np.concatenate(starts)
+    gi = np.concatenate(groups_of)
+    tasks["eb"] = gi
+    tasks["start"] = st
+    row_end = np.where(L[gi] >= TASK_COLUMNS, (st // L[gi] + 1) * L[gi], ncols[gi])
+    tasks["count"] = np.minimum(np.minimum(per[gi], row_end - st), ncols[gi] - st)
+    return tasks
 
 
 def emulate(gtab, pieces, tasks, U, src, out):

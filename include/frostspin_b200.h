@@ -123,10 +123,14 @@ int fs_abelian_permute(const double* d_in, int64_t in_len, double* d_out,
  * input piece with base < 0 is an absent source block (zeros).  Pieces
  * in_first .. in_first + in_count - 1 are the group's inputs, out_first .. its
  * outputs.  Tasks are FsPermTask with eb = group index, start = first column,
- * count = number of columns.  Limits: fs_su2_fused_limits.  Accesses outside
- * a buffer are skipped and raise FS_ERR_BOUNDS in *d_flag (if not null).
+ * count = number of columns; the columns of a task span at most
+ * FS_SU2_TASK_ROWS values of the outer legs (all legs but the innermost), a
+ * task that spans more is skipped and flagged.  Limits: fs_su2_fused_limits.
+ * Accesses outside a buffer are skipped and raise FS_ERR_BOUNDS in *d_flag (if
+ * not null).
  */
 #define FS_SU2_MAXD 8
+#define FS_SU2_TASK_ROWS 48
 
 typedef struct FsSu2Group {
     int64_t u_off;

@@ -72,31 +72,39 @@ def test_transfer_spectrum_and_corr_length_match_reference(tag):
         assert abs(xv - float(ref[f"{tag}_xi_v{k}"])) < 1e-7 * float(ref[f"{tag}_xi_v{k}"])
 
 
-def test_su2_ctmrg_from_reference_d24_tensors():
+@pytest.mark.parametrize("fused", [False, True])
+def test_su2_ctmrg_from_reference_d24_tensors(fused):
     """SU(2) SequentialCTMRG on the benchmark's site tensors (the reference's
     own D=24 simple update at beta=2, Dmax=28) at chi=24: chi after each
     iteration (bit-identical truncation), rdms and energy against the
-    reference's run."""
+    reference's run; with the SU(2) permutes through the three launches and
+    through the fused kernel."""
     from frostspin_b200 import SU2SymmetricTensor
     from frostspin_b200.ctmrg import SequentialCTMRG
+    from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
 
     d = load("su2_d24_beta2")
     ref = load("ctmrg_su2_d24")
     tensors = [SU2SymmetricTensor.load_from_dic(d, prefix=p) for p in ("A0", "A1")]
-    ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 24, cutoff=1e-10,
-                                                  degen_ratio=0.9999)
-    for it in range(2):
-        ctm.iterate()
-        assert np.array_equal(ctm.chi_values, ref[f"it{it}_chi"])
-    sds = np.array([[0.25, 0, 0, 0], [0, -0.25, 0.5, 0], [0, 0.5, -0.25, 0],
-                    [0, 0, 0, 0.25]]).reshape(2, 2, 2, 2)
-    es = []
-    for x, y in ctm.site_coords:
-        r12 = ctm.compute_rdm1x2(x, y).toarray()
-        r21 = ctm.compute_rdm2x1(x, y).toarray()
-        assert np.abs(r12 - ref[f"rdm1x2_{x}{y}"]).max() < 1e-9
-        assert np.abs(r21 - ref[f"rdm2x1_{x}{y}"]).max() < 1e-9
-        es += [np.einsum("ijkl,klij->", r12, sds), np.einsum("ijkl,klij->", r21, sds)]
+    was = lg.fused_permute_enabled()
+    lg.set_fused_permute(fused)
+    try:
+        ctm = SequentialCTMRG.from_elementary_tensors("AB\nBA", tensors, 24, cutoff=1e-10,
+                                                      degen_ratio=0.9999)
+        for it in range(2):
+            ctm.iterate()
+            assert np.array_equal(ctm.chi_values, ref[f"it{it}_chi"])
+        sds = np.array([[0.25, 0, 0, 0], [0, -0.25, 0.5, 0], [0, 0.5, -0.25, 0],
+                        [0, 0, 0, 0.25]]).reshape(2, 2, 2, 2)
+        es = []
+        for x, y in ctm.site_coords:
+            r12 = ctm.compute_rdm1x2(x, y).toarray()
+            r21 = ctm.compute_rdm2x1(x, y).toarray()
+            assert np.abs(r12 - ref[f"rdm1x2_{x}{y}"]).max() < 1e-9
+            assert np.abs(r21 - ref[f"rdm2x1_{x}{y}"]).max() < 1e-9
+            es += [np.einsum("ijkl,klij->", r12, sds), np.einsum("ijkl,klij->", r21, sds)]
+    finally:
+        lg.set_fused_permute(was)
     assert abs(np.mean(es) - float(ref["energy"])) < 1e-10
 
 

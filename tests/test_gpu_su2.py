@@ -56,18 +56,28 @@ def permute_cases(d, base):
         i += 1
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("base", ["sds", "sdsb", "ext", "miss", "r5", "r6"])
-def test_su2_permute_matches_reference(base):
+def test_su2_permute_matches_reference(base, fused):
+    """Every permute case of the reference's tensors, through the three
+    launches and through the fused kernel."""
+    from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
+
     d = load("su2")
     t = su2_from(d, base)
     n = 0
-    for pre, ra, ca in permute_cases(d, base):
-        p = t.permute(ra, ca)
-        check_against(p, d, pre)
-        if pre + "_dense" in d:
-            dense = d[pre + "_dense"]
-            assert np.abs(p.toarray() - dense).max() <= TOL * max(np.abs(dense).max(), 1)
-        n += 1
+    was = lg.fused_permute_enabled()
+    lg.set_fused_permute(fused)
+    try:
+        for pre, ra, ca in permute_cases(d, base):
+            p = t.permute(ra, ca)
+            check_against(p, d, pre)
+            if pre + "_dense" in d:
+                dense = d[pre + "_dense"]
+                assert np.abs(p.toarray() - dense).max() <= TOL * max(np.abs(dense).max(), 1)
+            n += 1
+    finally:
+        lg.set_fused_permute(was)
     assert n >= 2
 
 
@@ -177,15 +187,16 @@ def test_su2_cast_to_u1():
 
 @pytest.mark.parametrize("fused", [True, False])
 def test_su2_native_kernels_launched(fused):
-    """The SU(2) permute runs through the C-ABI: with the fused kernel one
-    launch takes the simple blocks with small recoupling matrices; without it
-    (the default), gather, recoupling GEMM and scatter launches.  Both give
-    the reference's blocks."""
+    """The SU(2) permute runs through the C-ABI: with the fused kernel (the
+    default) one launch takes the simple blocks with small recoupling
+    matrices; without it, gather, recoupling GEMM and scatter launches.  Both
+    give the reference's blocks."""
     from frostspin_b200 import _native
     from frostspin_b200.symmetric_tensor import lie_group_symmetric_tensor as lg
 
     d = load("su2")
     t = su2_from(d, "r5")
+    was = lg.fused_permute_enabled()
     lg.set_fused_permute(fused)
     try:
         before = dict(_native.CALL_COUNTS)
@@ -194,7 +205,7 @@ def test_su2_native_kernels_launched(fused):
         lg.set_fused_permute(not fused)
         q = t.permute((3, 0, 2), (1, 4))
     finally:
-        lg.set_fused_permute(False)
+        lg.set_fused_permute(was)
 
     def delta(*names):
         return sum(after.get(k, 0) - before.get(k, 0) for k in names)

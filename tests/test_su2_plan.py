@@ -89,10 +89,11 @@ def permute_cases(d):
 @pytest.fixture(params=["fused", "three_launch"])
 def fused_mode(request):
     """Permute maps built with the fused kernel for the thin simple blocks
-    and without it (the default)."""
+    (the default) and without it."""
+    was = lg.fused_permute_enabled()
     lg.set_fused_permute(request.param == "fused")
     yield request.param
-    lg.set_fused_permute(False)
+    lg.set_fused_permute(was)
 
 
 @pytest.mark.parametrize("trans", [False, True])
