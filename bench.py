@@ -248,7 +248,7 @@ def tensor_ops_ozaki(p, t2, precision):
 
 def mixed_kernel_names(precision):
     if precision.startswith("ozaki2_"):
-        return "k_oz_pair<CRT> (+ k_oz2_split, k_oz2_exponents)"
+        return "k_oz_pair<CRT>"
     return "k_oz_pair / k_oz_gemm (+ k_oz_split, k_oz_exponents)"
 
 
@@ -384,6 +384,18 @@ def timed_iterations(ctm, steps, precision, local):
     return s.elapsed_time(e) * 1e-3, clk, kernels, launches
 
 
+def _split_roofline(sp, hbm):
+    """The Ozaki II operand split (k_oz2_exponents + k_oz2_split) against the
+    copy bandwidth: per operand entry 8 bytes read twice (row maxima, then the
+    split) and one residue byte written per modulus."""
+    if not sp or not sp.get("ms"):
+        return None
+    gbs = sp["bytes"] / (sp["ms"] * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_oz2_exponents + k_oz2_split", "achieved": gbs,
+            "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "launches": sp["launches"],
+            "ms": sp["ms"]}
+
+
 def _fused_roofline(fz, hbm):
     """The fused SU(2) permute (k_su2_fused) against the copy bandwidth: 16
     bytes per coefficient (one read, one write)."""
@@ -428,7 +440,10 @@ def run_ctmrg(args, world, rank, local):
 
         n_cls, t_tune = autotune.tune(records, mixed)
         autotune.set_enabled(True)
+        pred = autotune.predict(records, mixed)
         tune_info = {"classes_measured": n_cls, "seconds": t_tune,
+                     "predicted_gemm_s_per_warmup_iteration": {
+                         k: v / max(args.warmup, 1) for k, v in pred.items()},
                      "classes_mixed": sum(1 for (m, _), r in autotune.table().items()
                                           if m == mixed and r["mixed"] < r["fp64"]),
                      "classes_total": sum(1 for (m, _) in autotune.table() if m == mixed)}
@@ -597,6 +612,7 @@ def run_ctmrg(args, world, rank, local):
                              "peak": hbm, "unit": "GB/s", "frac": perm_gbs / hbm,
                              "launches": perm["launches"], "ms": perm["ms"]},
         "roofline_permute_fused": _fused_roofline(kern.get("permute_fused"), hbm),
+        "roofline_ozaki_split": _split_roofline(kern.get("ozaki_split"), hbm),
         "e2e": {"value": world * e2e_steps / t_e2e, "unit": "iter/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "same_config_points": same_cfg,

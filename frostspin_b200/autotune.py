@@ -169,3 +169,32 @@ def decide(arr, mode, *, max_dist=2):
             memo[key] = _choice(mode, key, max_dist)
         out.append(memo[key])
     return out
+
+
+def predict(records, mode):
+    """Seconds the recorded launches would take by the measured rates: every
+    problem on FP64, every problem on the mixed path, and each on the path
+    decide() picks (problems of classes with no measured neighbour count on
+    FP64 in all three)."""
+    out = {"fp64": 0.0, "mixed": 0.0, "chosen": 0.0}
+    for arr in records:
+        M = arr["M"].astype(np.float64)
+        N = arr["N"].astype(np.float64)
+        K = arr["K"].astype(np.float64)
+        flops = 2.0 * M * N * K
+        for i in range(arr.size):
+            key = shape_class(arr["M"][i], arr["N"][i], arr["K"][i])
+            row = _TABLE.get((mode, key))
+            if row is None:
+                near = [r for (m, k), r in _TABLE.items() if m == mode and
+                        sum(abs(a - b) for a, b in zip(k, key, strict=True)) <= 2]
+                row = min(near, key=lambda r: sum(abs(a - b) for a, b in zip(
+                    shape_class(*r["shape"]), key, strict=True))) if near else None
+            if row is None:
+                continue
+            f64, mx = row["fp64"] * flops[i], row["mixed"] * flops[i]
+            out["fp64"] += f64
+            out["mixed"] += mx
+            out["chosen"] += min(f64, mx)
+    return out
+

@@ -222,9 +222,9 @@ def grouped_gemm(problems):
         else:
             use = fits & _tuned(arr, mode, ozaki2_pays(arr, nmod))
         if use.any():
-            with instrument.region("gemm_ozaki", flops=float(flops[use].sum()),
-                                   int8_ops=ozaki2_int8_ops(arr[use], nmod)):
-                ozaki2_gemm(arr[use], nmod)
+            # regions inside: the split kernels and the tcgen05 GEMM apart
+            ozaki2_gemm(arr[use], nmod, flops=float(flops[use].sum()),
+                        int8_ops=ozaki2_int8_ops(arr[use], nmod))
         if (~use).any():
             with instrument.region("gemm_fp64", flops=float(flops[~use].sum())):
                 _dgemm(arr[~use], None, tm, tn, ntile[~use])
@@ -721,10 +721,12 @@ def ozaki2_plan(arr, nmod):
 _OZ2_SCRATCH = {}
 
 
-def ozaki2_gemm(arr, nmod):
+def ozaki2_gemm(arr, nmod, *, flops=0.0, int8_ops=0.0):
     """Run the problems of `arr` (GEMM_PROBLEM_DTYPE) on the Ozaki II path
     (fs_ozaki2_split + fs_ozaki2_gemm_pair); the slice workspace and the CRT
-    scratch come from torch's caching allocator."""
+    scratch come from torch's caching allocator.  Instrumented as two
+    regions: "ozaki_split" (exponent and residue-slice kernels, 8 + 8 bytes
+    read and nmod written per operand entry) and "gemm_ozaki" (the GEMM)."""
     ops, probs, tiles, nbytes = ozaki2_plan(arr, nmod)
     if tiles.size == 0:
         return None
@@ -743,14 +745,17 @@ def ozaki2_gemm(arr, nmod):
     d_tiles = dev.upload(tiles)
     max_rows = int(ops["rows"].max())
     max_units = int((ops["rowtiles"].astype(np.int64) * 4 * ops["ktiles"]).max())
-    for start in range(0, ops.size, 65534):
-        cnt = min(65534, ops.size - start)
-        _native.call("fs_ozaki2_split", d_ops.data_ptr() + start * ops.itemsize, cnt, max_rows,
-                     max_units, nmod, dev.stream())
+    entries = float((ops["rows"].astype(np.float64) * ops["K"]).sum())
+    with instrument.region("ozaki_split", bytes=entries * (16 + nmod)):
+        for start in range(0, ops.size, 65534):
+            cnt = min(65534, ops.size - start)
+            _native.call("fs_ozaki2_split", d_ops.data_ptr() + start * ops.itemsize, cnt,
+                         max_rows, max_units, nmod, dev.stream())
     flag = torch.zeros(1, dtype=torch.int32, device=dev.device())
-    _native.call("fs_ozaki2_gemm_pair", d_probs.data_ptr(), probs.size, d_tiles.data_ptr(),
-                 tiles.size, nmod, base, ws_bytes, base + ws_bytes, scratch_bytes,
-                 flag.data_ptr(), dev.stream())
+    with instrument.region("gemm_ozaki", flops=flops, int8_ops=int8_ops):
+        _native.call("fs_ozaki2_gemm_pair", d_probs.data_ptr(), probs.size, d_tiles.data_ptr(),
+                     tiles.size, nmod, base, ws_bytes, base + ws_bytes, scratch_bytes,
+                     flag.data_ptr(), dev.stream())
     _OZ_FLAGS.append(flag)
     if len(_OZ_FLAGS) > 64:
         check_ozaki_flags()

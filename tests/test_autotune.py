@@ -59,3 +59,23 @@ def test_unmeasured_classes_take_nearest_measured_choice():
         assert mid == (12, 12, 12)
     finally:
         autotune.clear()
+
+
+def test_predict_sums_measured_rates():
+    autotune.clear()
+    mode = "ozaki2_11"
+    big = (3000, 3000, 3000)
+    thin = (100, 5000, 40)
+    autotune._TABLE[(mode, autotune.shape_class(*big))] = {"fp64": 3e-14, "mixed": 1e-14,
+                                                           "shape": big}
+    autotune._TABLE[(mode, autotune.shape_class(*thin))] = {"fp64": 1e-13, "mixed": 4e-13,
+                                                            "shape": thin}
+    try:
+        rec = [_arr([big, thin, (7, 7, 7)])]
+        got = autotune.predict(rec, mode)
+        fb, ft = 2.0 * 3000**3, 2.0 * 100 * 5000 * 40
+        assert abs(got["fp64"] - (3e-14 * fb + 1e-13 * ft)) < 1e-12
+        assert abs(got["mixed"] - (1e-14 * fb + 4e-13 * ft)) < 1e-12
+        assert abs(got["chosen"] - (1e-14 * fb + 1e-13 * ft)) < 1e-12
+    finally:
+        autotune.clear()
