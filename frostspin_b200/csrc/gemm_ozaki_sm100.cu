@@ -1108,10 +1108,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 // Thread mapping: a block handles a 32-row group of one k-tile (32 rows x 128
 // k values); each thread 16 consecutive k of one row.  When the operand's rows
 // are contiguous in memory (transposed storage) a warp spans 32 rows at one
-// k-chunk, otherwise 4 rows x 8 chunks, so both layouts read coalesced.
+// k-chunk and reads them directly, coalesced.  Otherwise (k contiguous) the
+// block first copies the 32 x 128 tile into shared memory with consecutive
+// threads on consecutive k (a thread's own 16 k would spread one warp load over
+// 32 sectors), each 16-value chunk padded to 17 doubles so that the threads of
+// a half warp read 16 distinct bank pairs.
+constexpr int kSplitPad = 17;
+
 __global__ void __launch_bounds__(256)
     k_oz2_split(const FsOz2Operand* __restrict__ ops, int64_t n_ops,
                 const __grid_constant__ CrtConsts cc) {
+    __shared__ double stage[32 * 8 * kSplitPad];
     const int op_id = blockIdx.y;
     if (op_id >= n_ops) return;
     const FsOz2Operand op = ops[op_id];
@@ -1132,13 +1139,33 @@ __global__ void __launch_bounds__(256)
         const int64_t k0 = static_cast<int64_t>(kt) * kTileK + c * 16;
         const bool row_ok = row < op.rows;
         const int sh = op.bits - (row_ok ? op.exps[row] : 0);
+        if (!rows_contiguous) {
+            // coalesced copy of the block's 32 rows x 128 k into shared memory
+            const int64_t row_base = static_cast<int64_t>(rt) * kSplitRows +
+                                     (rg % (kSplitRows / 32)) * 32;
+            const int64_t kb = static_cast<int64_t>(kt) * kTileK;
+            __syncthreads();   // the previous unit's reads of the stage are done
+#pragma unroll
+            for (int it = 0; it < 16; ++it) {
+                const int e = it * 256 + t;
+                const int sr = e >> 7, sk = e & 127;
+                const int64_t grow = row_base + sr, gk = kb + sk;
+                stage[(sr * 8 + (sk >> 4)) * kSplitPad + (sk & 15)] =
+                    (grow < op.rows && gk < op.K) ? __ldg(op.src + grow * op.s_row + gk * op.s_k)
+                                                  : 0.0;
+            }
+            __syncthreads();
+        }
         int32_t lo[16];
         double ad[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int64_t k = k0 + j;
-            const double x =
-                (row_ok && k < op.K) ? __ldg(op.src + row * op.s_row + k * op.s_k) : 0.0;
+            double x;
+            if (rows_contiguous)
+                x = (row_ok && k < op.K) ? __ldg(op.src + row * op.s_row + k * op.s_k) : 0.0;
+            else
+                x = stage[(r * 8 + c) * kSplitPad + j];
             const double tt = scale2(x, sh) + kRoundMagic;
             lo[j] = __double2loint(tt);
             ad[j] = tt - kRoundMagic;
