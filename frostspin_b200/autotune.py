@@ -57,7 +57,10 @@ def table():
     return dict(_TABLE)
 
 
-def _time_launch(M, N, K, ta, tb, copies, mode, reps):
+def _time_launch(M, N, K, ta, tb, copies, modes, reps):
+    """Best time of `reps` launches of the class on each path of `modes`, after
+    one untimed launch each; the paths alternate launch by launch, so that a
+    clock or power drift during the measurement affects them alike."""
     from . import linalg
 
     g = torch.Generator(device=dev.device())
@@ -69,19 +72,20 @@ def _time_launch(M, N, K, ta, tb, copies, mode, reps):
         dC = torch.empty(M * N, dtype=torch.float64, device=dev.device())
         specs.append({"A": dA, "a_off": 0, "a_trans": ta, "B": dB, "b_off": 0, "b_trans": tb,
                       "C": dC, "c_off": 0, "M": M, "N": N, "K": K})
-    best = float("inf")
+    best = {m: float("inf") for m in modes}
     for r in range(reps + 1):
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        with linalg.gemm_precision_mode(mode), linalg.ozaki_dispatch_mode("all"), \
-                _bypass():
-            linalg.grouped_gemm(specs)
-        e1.record()
-        torch.cuda.synchronize()
-        if r:
-            best = min(best, e0.elapsed_time(e1) * 1e-3)
+        for mode in modes:
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            with linalg.gemm_precision_mode(mode), linalg.ozaki_dispatch_mode("all"), \
+                    _bypass():
+                linalg.grouped_gemm(specs)
+            e1.record()
+            torch.cuda.synchronize()
+            if r:
+                best[mode] = min(best[mode], e0.elapsed_time(e1) * 1e-3)
     linalg.check_ozaki_flags()
     return best
 
@@ -97,7 +101,7 @@ class _bypass:
         _ENABLED["on"] = self.old
 
 
-def tune(records, mode, *, reps=2, min_flops=1e8):
+def tune(records, mode, *, reps=3, min_flops=1e8):
     """Measure every shape class of the recorded launches (a list of
     GEMM_PROBLEM_DTYPE tables) not measured yet for `mode`; returns the number
     of classes measured and the seconds spent."""
@@ -125,11 +129,9 @@ def tune(records, mode, *, reps=2, min_flops=1e8):
         per_copy = 8 * (M * K + K * Nc + M * Nc)
         copies = int(max(1, min(-(-_TARGET_TILES // tiles), _MAX_BYTES // max(per_copy, 1))))
         flops = 2.0 * M * Nc * K * copies
-        row = {"shape": (M, N, K), "copies": copies}
-        for path in ("fp64", mode):
-            row["fp64" if path == "fp64" else "mixed"] = (
-                _time_launch(M, Nc, K, ta, tb, copies, path, reps) / flops)
-        _TABLE[(mode, key)] = row
+        t = _time_launch(M, Nc, K, ta, tb, copies, ("fp64", mode), reps)
+        _TABLE[(mode, key)] = {"shape": (M, N, K), "copies": copies,
+                               "fp64": t["fp64"] / flops, "mixed": t[mode] / flops}
         n += 1
     return n, time.perf_counter() - t0
 

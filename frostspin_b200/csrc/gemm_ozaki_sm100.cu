@@ -1115,7 +1115,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 // a half warp read 16 distinct bank pairs.
 constexpr int kSplitPad = 17;
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_oz2_split(const FsOz2Operand* __restrict__ ops, int64_t n_ops,
                 const __grid_constant__ CrtConsts cc) {
     __shared__ double stage[32 * 8 * kSplitPad];
@@ -1156,39 +1156,45 @@ __global__ void __launch_bounds__(256)
             }
             __syncthreads();
         }
-        int32_t lo[16];
-        double ad[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int64_t k = k0 + j;
-            double x;
-            if (rows_contiguous)
-                x = (row_ok && k < op.K) ? __ldg(op.src + row * op.s_row + k * op.s_k) : 0.0;
-            else
-                x = stage[(r * 8 + c) * kSplitPad + j];
-            const double tt = scale2(x, sh) + kRoundMagic;
-            lo[j] = __double2loint(tt);
-            ad[j] = tt - kRoundMagic;
-        }
         int8_t* dst = op.slices + (static_cast<int64_t>(kt) * op.rowtiles + rt) * kABytes +
                       rr * 128 + ((c ^ (rr & 7)) * 16);
-        {
-            uint32_t w[4] = {0, 0, 0, 0};
+        // the 16 k of this thread in two halves of 8 (8-byte stores per
+        // modulus): half the live operand registers, so that three CTAs fit on
+        // an SM without spills
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-                w[j / 4] |= (static_cast<uint32_t>(lo[j]) & 0xFFu) << (8 * (j % 4));
-            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-        for (int m = 1; m < n; ++m) {
-            const int32_t pm = cc.p[m];
-            const double ipm = cc.inv_p[m];
-            uint32_t w[4] = {0, 0, 0, 0};
+        for (int h = 0; h < 2; ++h) {
+            int32_t lo[8];
+            double ad[8];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int32_t q = __double2loint(fma(ad[j], ipm, kRoundMagic));
-                w[j / 4] |= (static_cast<uint32_t>(lo[j] - q * pm) & 0xFFu) << (8 * (j % 4));
+            for (int j = 0; j < 8; ++j) {
+                const int64_t k = k0 + 8 * h + j;
+                double x;
+                if (rows_contiguous)
+                    x = (row_ok && k < op.K) ? __ldg(op.src + row * op.s_row + k * op.s_k) : 0.0;
+                else
+                    x = stage[(r * 8 + c) * kSplitPad + 8 * h + j];
+                const double tt = scale2(x, sh) + kRoundMagic;
+                lo[j] = __double2loint(tt);
+                ad[j] = tt - kRoundMagic;
             }
-            *reinterpret_cast<uint4*>(dst + m * slice_stride) = make_uint4(w[0], w[1], w[2], w[3]);
+            {
+                uint32_t w[2] = {0, 0};
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    w[j / 4] |= (static_cast<uint32_t>(lo[j]) & 0xFFu) << (8 * (j % 4));
+                *reinterpret_cast<uint2*>(dst + 8 * h) = make_uint2(w[0], w[1]);
+            }
+            for (int m = 1; m < n; ++m) {
+                const int32_t pm = cc.p[m];
+                const double ipm = cc.inv_p[m];
+                uint32_t w[2] = {0, 0};
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int32_t q = __double2loint(fma(ad[j], ipm, kRoundMagic));
+                    w[j / 4] |= (static_cast<uint32_t>(lo[j] - q * pm) & 0xFFu) << (8 * (j % 4));
+                }
+                *reinterpret_cast<uint2*>(dst + m * slice_stride + 8 * h) = make_uint2(w[0], w[1]);
+            }
         }
     }
 }
