@@ -653,14 +653,16 @@ def fixture_site_tensors(symmetry):
     return out
 
 
-def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1):
+def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1, one_thread=True):
     """Bounded CPU sample of the CTMRG workload: the numpy oracle (restating the
     reference) from the reference's own site tensors, with BLAS on every host
     core (pinned through threadpoolctl); at each chi of `chis` one untimed
     iteration grows the environment to that chi, then `timed` iterations are
     timed.  The value at chi_target is a power law t = t(chis[-1]) (chi /
     chis[-1])^p fitted on the last two measured points, labelled as an
-    extrapolation when chi_target is not among them."""
+    extrapolation when chi_target is not among them.  With one_thread, one more
+    iteration of the first chi's environment is timed with BLAS on one thread
+    (the 1-thread number of the baseline protocol)."""
     from threadpoolctl import threadpool_info, threadpool_limits
 
     from oracle import ctmrg_oracle as co
@@ -668,6 +670,7 @@ def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1):
     cores = os.cpu_count() or 1
     A, B = fixture_site_tensors(symmetry)
     times = {}
+    first_env = None
     with threadpool_limits(limits=cores):
         threads = sorted({int(d.get("num_threads", 0)) for d in threadpool_info()})
         for chi in chis:
@@ -677,6 +680,14 @@ def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1):
             for _ in range(timed):
                 c.iterate()
             times[chi] = (time.perf_counter() - t0) / timed
+            if first_env is None:
+                first_env = c
+    one = None
+    if one_thread and first_env is not None:
+        with threadpool_limits(limits=1):
+            t0 = time.perf_counter()
+            first_env.iterate()
+            one = {"chi": int(chis[0]), "s_per_iter": time.perf_counter() - t0, "threads": 1}
     measured = chi_target in times
     if measured:
         t_target, p = times[chi_target], None
@@ -696,6 +707,7 @@ def cpu_ctmrg_sample(symmetry, chi_target, *, chis=(32, 64), timed=1):
                       f"extrapolated to chi={chi_target} ({t_target:.0f} s/iteration), "
                       f"labelled as an extrapolation")),
         "measured_s_per_iter": {str(k): v for k, v in times.items()},
+        "one_thread": one,
         "fit_exponent": p, "extrapolated": not measured,
     }
 
