@@ -228,3 +228,28 @@ def test_su2_permute_tables_random_against_oracle(seed):
         for o, (r, c), b in zip(m.out_offsets, m.out_shapes, ref.blocks, strict=True):
             assert (r, c) == b.shape
             assert np.abs(out[o : o + r * c].reshape(r, c) - b).max() <= TOL * scale
+
+
+@pytest.mark.parametrize("dims", [(), (7,), (3, 5), (2, 9000), (5, 10, 3), (4, 1, 6, 2), (300, 40)])
+def test_fused_tasks_cover_columns_within_row_limit(dims):
+    """make_tasks: every column of a group in exactly one task, no task spans
+    more than TASK_ROWS values of the outer legs, and a row longer than
+    TASK_COLUMNS is cut inside the row (the kernel skips and flags a task
+    that spans more rows)."""
+    from frostspin_b200._native import SU2_GROUP_DTYPE
+    from frostspin_b200.symmetric_tensor import su2_fused_plan as sp
+
+    g = np.zeros(1, dtype=SU2_GROUP_DTYPE)
+    g["ndim"] = len(dims)
+    g["dims"] = 1
+    g["dims"][0, : len(dims)] = dims
+    n = int(np.prod(dims)) if dims else 1
+    g["ncols"] = n
+    t = sp.make_tasks(g)
+    L = dims[-1] if dims else 1
+    cols = np.concatenate([np.arange(s, s + c) for s, c in zip(t["start"], t["count"], strict=True)])
+    assert np.array_equal(np.sort(cols), np.arange(n))
+    for s, c in zip(t["start"].astype(np.int64), t["count"].astype(np.int64), strict=True):
+        assert c >= 1
+        assert (s + c - 1) // L - s // L + 1 <= sp.TASK_ROWS
+        assert c <= max(sp.TASK_COLUMNS, L * sp.TASK_ROWS)
