@@ -1107,6 +1107,49 @@ def run_ising(args, world, rank, local):
     return line
 
 
+def cpu_simple_update_sample(symmetry, D, warmup, *, budget_s=15.0):
+    """Bounded CPU sample of the simple-update workload: the numpy oracle
+    (restating the reference) on the same model, from the same infinite-
+    temperature start; the first cycle and `warmup` more untimed, then cycles
+    (evolve(4 tau) each, as on the device) timed until `budget_s` has passed
+    (at least three), with BLAS on every host core, then two cycles on one
+    BLAS thread."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import frostspin_oracle as fo
+    from oracle import simple_update_oracle as suo
+    from oracle import su2_oracle as so
+
+    cores = os.cpu_count() or 1
+    if symmetry == "su2":
+        r = np.array([[1], [2]])
+        h = so.from_array(SDS_22.reshape(2, 2, 2, 2), (r, r), (r, r))
+    else:
+        rep = np.array([1, -1], dtype=np.int8)
+        h = fo.from_array(SDS_22.reshape(2, 2, 2, 2), (rep, rep), (rep, rep))
+    cycle = 4 * 0.01
+    with threadpool_limits(limits=cores):
+        su = suo.SimpleUpdate(h, D, 0.01, rcutoff=1e-10, degen_ratio=0.9999)
+        for _ in range(1 + warmup):
+            su.evolve(cycle)
+        n, t0 = 0, time.perf_counter()
+        while n < 3 or time.perf_counter() - t0 < budget_s:
+            su.evolve(cycle)
+            n += 1
+        t = time.perf_counter() - t0
+    with threadpool_limits(limits=1):
+        t1 = time.perf_counter()
+        for _ in range(2):
+            su.evolve(cycle)
+        one = (time.perf_counter() - t1) / 2
+    return {"value": n / t, "unit": "cycle/s", "cores": cores, "kind": "port",
+            "sample": (f"numpy oracle simple update ({symmetry}, D={D} target, tau=0.01) from "
+                       f"beta=0: {1 + warmup} untimed cycles, then {n} timed cycles in "
+                       f"{t:.1f} s with BLAS on {cores} host cores (beta "
+                       f"{(1 + warmup) * cycle:.2f} to {(1 + warmup + n) * cycle:.2f})"),
+            "one_thread": {"s_per_cycle": one, "threads": 1}}
+
+
 def run_simple_update(args, world, rank, local):
     """Config 3: the SU(2) finite-temperature simple update of the spin-1/2
     Heisenberg model (2-site checkerboard cell, second-order Trotter, tau =
@@ -1158,6 +1201,8 @@ def run_simple_update(args, world, rank, local):
                    "l2": "bond tensors of a few MB: L2-resident, launch-bound",
                    "parallelism": f"replicas x{world}"},
         "clocks": clk,
+        **({"cpu_baseline": cpu_simple_update_sample(args.symmetry, args.D, args.warmup)}
+           if rank == 0 and world == 1 and not args.no_cpu_baseline else {}),
     }
 
 
@@ -1363,6 +1408,19 @@ def run_reference(args, world, rank):
                 "config": {"workload": "batched_ising_c4v", "runs": BATCH_RUNS},
                 "cpu_baseline": info,
                 "e2e": {"value": v, "unit": "run-iter/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    if args.workload == "simple_update":
+        info = cpu_simple_update_sample(args.symmetry, args.D, args.warmup)
+        v = info["value"]
+        return {"metric": "SU(2) simple update Trotter cycles/s (D=24 target)", "value": v,
+                "unit": "cycle/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (infinite-temperature start)", "impl": "reference",
+                "config": {"workload": "simple_update_" + args.symmetry, "D_target": args.D,
+                           "tau": 0.01},
+                "cpu_baseline": info,
+                "e2e": {"value": v, "unit": "cycle/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
     if args.workload == "ising":
         info = cpu_ising_sample(max(args.steps, 20))

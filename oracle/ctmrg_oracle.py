@@ -1,5 +1,5 @@
-"""CPU oracle of the double-layer SequentialCTMRG and of the simple update --
-TEST INFRASTRUCTURE ONLY.
+"""CPU oracle of the double-layer SequentialCTMRG (the simple update is in
+simple_update_oracle.py) -- TEST INFRASTRUCTURE ONLY.
 
 A numpy restatement of frostspin/ctmrg (ctm_contract.py, ctm_renormalize.py,
 ctm_environment.py, sequential_ctmrg.py, rdm.py) on the oracle tensors of
