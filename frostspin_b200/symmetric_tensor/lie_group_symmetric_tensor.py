@@ -433,8 +433,8 @@ class LieGroupSymmetricTensor(NonAbelianSymmetricTensor):
         _, ci = cls._fuse_elementary(irr[nrr:])
         _, ro = cls._fuse_elementary(irr_out[:new_nrr])
         _, co = cls._fuse_elementary(irr_out[new_nrr:])
-        shared_in = tuple(int(x) for x in np.intersect1d(ri, ci))
-        shared_out = tuple(int(x) for x in np.intersect1d(ro, co))
+        shared_in = tuple(sorted(set(ri.tolist()) & set(ci.tolist())))
+        shared_out = tuple(sorted(set(ro.tolist()) & set(co.tolist())))
         tri = cls.elementary_trees(irr[:nrr], tuple(bool(s) for s in sig[:nrr]), shared_in)
         tci = cls.elementary_trees(irr[nrr:], tuple(bool(s) for s in ~sig[nrr:]), shared_in)
         tro = cls.elementary_trees(
@@ -450,20 +450,24 @@ class LieGroupSymmetricTensor(NonAbelianSymmetricTensor):
         perm[:ndim] = (ax >= nrr) + ax
         perm[ndim] = nrr
         perm[ndim + 1] = ndim + 1
-        cols = []
+        n_rows = sum(op.shape[0] for op in out_proj)
+        n_cols = sum(tri[b].shape[-2] * tci[b].shape[-2] for b in shared_in)
+        u = np.empty((n_rows, n_cols))
+        c0 = 0
         for b in shared_in:
             rtree, ctree = tri[b], tci[b]
             d = rtree.shape[-1]
             p = rtree.reshape(-1, d) @ ctree.reshape(-1, d).T
             p = p.reshape(rtree.shape[:-1] + ctree.shape[:-1]).transpose(perm)
-            p = p.reshape(-1, rtree.shape[-2] * ctree.shape[-2])
-            parts = []
+            w = rtree.shape[-2] * ctree.shape[-2]
+            p = p.reshape(-1, w)
+            r0 = 0
             for op, dim in zip(out_proj, dims_out, strict=True):
                 iso = op @ p
                 iso[np.abs(iso) < 1e-14] = 0
-                parts.append(iso / dim)
-            cols.append(np.vstack(parts))
-        u = np.ascontiguousarray(np.hstack(cols))
+                u[r0 : r0 + iso.shape[0], c0 : c0 + w] = iso / dim
+                r0 += iso.shape[0]
+            c0 += w
         u.setflags(write=False)
         cls._iso_cache[key] = u
         return u
