@@ -144,3 +144,31 @@ def test_task_tables_cover_every_row_once():
             assert 1 <= t["count"] <= MAX_TASK_ROWS
             covered[t["eb"]] += t["count"]
         assert np.array_equal(covered, rows)
+
+
+def test_tile_runs_order_and_layout():
+    """The FsTileRun table of a DMMA launch (linalg._tile_runs): problems in the
+    given order with their tile counts as consecutive runs, wide problems
+    (more tile columns than rows) column-major, empty problems taking no
+    tiles; expanding it as fs_expand_tiles does enumerates every tile once."""
+    from frostspin_b200 import linalg
+
+    ncol = np.array([3, 4, 1, 2, 2, 5, 1], dtype=np.int64)
+    nrow = np.array([2, 0, 1, 6, 0, 1, 0], dtype=np.int64)
+    ntile = ncol * nrow
+    order = np.array([3, 1, 0, 6, 2, 5, 4])
+    runs, total = linalg._tile_runs(ntile, ncol, order, nrow)
+    assert total == int(ntile.sum())
+    assert list(runs["problem"]) == list(order)
+    assert list(runs["start"]) == list(np.cumsum(ntile[order]) - ntile[order])
+    assert list(runs["col_major"]) == [int(ncol[p] > nrow[p]) for p in order]
+    tiles = []
+    for t in range(total):
+        r = runs[np.searchsorted(runs["start"], t, side="right") - 1]
+        k = t - int(r["start"])
+        if r["col_major"]:
+            tiles.append((int(r["problem"]), k % int(r["nrow"]), k // int(r["nrow"])))
+        else:
+            tiles.append((int(r["problem"]), k // int(r["ncol"]), k % int(r["ncol"])))
+    assert sorted(tiles) == sorted((p, i, j) for p in range(7) for i in range(nrow[p])
+                                   for j in range(ncol[p]))
